@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark: Orszag-Tang cell-updates/s, FP32-bulk vs FP64, and HBM % of peak.
+
+Workload (one step = one split time step of the whole grid): the Orszag-Tang
+vortex on periodic [0,1]^2 at 4096^2 cells, HLLD, van Leer, CFL 0.4, GLM
+c_h = max wave speed, c_r = 0.18 -- deterministic synthetic initial data,
+generated by the library (no dataset).  The state (604 MB in FP32, 1.2 GB in
+FP64) is larger than the 126 MB L2, so no flush is needed between steps.
+
+Our arm:  `value` = FP32-bulk cell-updates/s of the device-resident, CUDA-graph
+step loop (mhd_run) with the state already in HBM, timed with CUDA events on
+the launching stream, max over ranks.  `e2e` = the same metric through the C
+ABI with pinned FP64 host buffers: every step uploads the state, advances one
+step and downloads the state.  The FP64 step is timed the same way and
+reported beside it with the FP32/FP64 speed ratio and the density relative L1
+between the two after the same steps.
+
+`--impl reference`: the reference's own CPU/OpenMP step (oracle/_ref, built
+from the reference sources) on the host cores, rank 0 only.
+
+Multi-GPU (torchrun): one independent instance per rank (weak scaling, no
+data-path collective); a barrier brackets the timed region and the time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Orszag–Tang cell-updates/s FP32-bulk vs FP64 at L1≤1e-5; HBM % of peak"
+UNIT = "cell-updates/s"
+BYTES_PER_CELL_SWEEP = {4: 2 * 9 * 4, 8: 2 * 9 * 8}  # read + write 9 fields per sweep
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4096, help="grid side")
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("timestamp,index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = (bus_id or "").lower()
+        self.proc = None
+        self.path = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-f", self.path], stdout=subprocess.DEVNULL,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.6)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def mark(self, which):
+        setattr(self, which, time.time())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 11:
+                    continue
+                if self.bus_id and self.bus_id[-12:] not in p[2].lower():
+                    continue
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+
+        def ts(s):
+            try:
+                return time.mktime(time.strptime(s.split(".")[0], "%Y/%m/%d %H:%M:%S"))
+            except ValueError:
+                return None
+
+        load = [r for r in rows if ts(r[0]) is not None and self.t0 - 1 <= ts(r[0]) <= self.t1 + 1] or rows
+        sm = [float(r[3]) for r in load if r[3].replace(".", "").isdigit()]
+        mx = [float(r[4]) for r in load if r[4].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in load for k in range(4) if r[7 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(load)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_reference_run(n: int, steps: int, warmup: int, budget_s: float | None):
+    """The reference's CPU step on this host: returns (per-step seconds list, threads)."""
+    import numpy as np
+
+    from mhd_gpu_acc_b200 import CaseId, get_n_case_config, initialise
+    from oracle.oracle import REF_SO, Reference
+
+    if not os.path.exists(REF_SO):
+        return None, 0, "reference CPU build oracle/_ref/libmhdref.so is missing"
+    ref = Reference()
+    threads = os.cpu_count() or 1
+    ref.set_threads(threads)
+    cfg = get_n_case_config(CaseId.OrszagTangUnit, 1)
+    U = initialise(CaseId.OrszagTangUnit, n, n, 2, cfg.extent)
+    bc = (0, 0, 0, 0)
+    if budget_s is not None:  # size the sample from one probe step
+        rc, k, secs, ch = ref.run_timed(U, 2, cfg.extent, cfg.gamma, cfg.cfl, 2, bc, 1, cfg.t_end)
+        per = float(secs[0])
+        steps = int(max(1, min(steps, budget_s / max(per, 1e-9))))
+        warmup = 0
+    rc, k, secs, ch = ref.run_timed(U, 2, cfg.extent, cfg.gamma, cfg.cfl, 2, bc, warmup + steps, cfg.t_end)
+    del U
+    if rc != 0 or k != warmup + steps:
+        return None, threads, f"reference run stopped early (rc {rc}, {k} steps)"
+    return list(np.asarray(secs[warmup:])), threads, None
+
+
+def run_reference_arm(a, world, rank):
+    if rank != 0:
+        return 0
+    n = a.n
+    secs, threads, err = cpu_reference_run(n, a.steps, a.warmup, None)
+    if err:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    tot = sum(secs)
+    value = n * n * len(secs) / tot
+    sample = (f"Orszag-Tang [0,1]^2 {n}x{n}, HLLD, minmod (the reference has no van Leer limiter; "
+              f"same cost class), CFL 0.4, {a.warmup} warm-up + {len(secs)} timed steps, FP64 AoS")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": len(secs),
+        "warmup": a.warmup, "ms_per_step": 1e3 * tot / len(secs), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (deterministic Orszag-Tang initial data)",
+        "config": {"workload": f"orszag_tang_unit_{n}x{n}_hlld_cfl0.4", "nx": n, "ny": n, "solver": "hlld",
+                   "limiter": "minmod", "precision": "fp64", "device": "host cpu (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(a, world, rank, local):
+    import numpy as np
+    import torch
+
+    import mhd_gpu_acc_b200 as m
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.Stream()
+    n = a.n
+    cfg = m.get_n_case_config(m.CaseId.OrszagTangUnit, 1)
+    solver, limiter, bc = m.RiemannSolver.HLLD, m.Limiter.VANLEER, m.BoundaryConfig(0, 0, 0, 0)
+    U0 = m.initialise(m.CaseId.OrszagTangUnit, n, n, 2, cfg.extent)
+    t_end = cfg.t_end
+    res = {}
+    states = {}
+
+    def arm(dtype):
+        U = m.Grid2DGPU(n, n, 2, *cfg.extent, dtype)
+        T = m.Grid2DGPU(n, n, 2, *cfg.extent, dtype)
+        ws = m.GpuWorkspace()
+        m.init_gpu_workspace(ws, U)
+        m.set_gpu_physics_gamma(ws, cfg.gamma)
+        m.set_gpu_physics_ch(ws, 0.0)
+        ws.set_limiter(limiter)
+        ws.set_stream(stream.cuda_stream)
+        U.upload(U0)
+        ws.run(U, T, cfg.cfl, t_end, a.warmup, solver, bc)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = m.launch_count()
+        sampler.mark("t0")
+        e0.record(stream)
+        info = ws.run(U, T, cfg.cfl, t_end, a.steps, solver, bc)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sampler.mark("t1")
+        launches = m.launch_count() - l0
+        barrier(world)
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        assert info.steps == a.steps, info.steps
+        prof = ws.profile_sweeps(U, T, cfg.cfl, t_end, solver, bc, 5)
+        states[dtype] = U.download()[0]
+        ws.destroy()
+        return dict(ms=ms, launches=launches, sweeps_ms=prof, t=info.t, fallbacks=info.fallbacks)
+
+    bus = None
+    try:
+        p = torch.cuda.get_device_properties(local)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}"
+    except Exception:
+        pass
+    sampler = ClockSampler(bus)
+    sampler.start()
+    res[m.F32] = arm(m.F32)
+    clocks = sampler.stop()
+    if not a.no_fp64:
+        res[m.F64] = arm(m.F64)
+
+    cells = n * n
+    v32 = world * cells * a.steps / (res[m.F32]["ms"] / 1e3)
+    out_fp64 = None
+    l1 = None
+    if m.F64 in res:
+        v64 = world * cells * a.steps / (res[m.F64]["ms"] / 1e3)
+        r64 = states[m.F64][2:-2, 2:-2]
+        l1 = float(np.abs(states[m.F32][2:-2, 2:-2] - r64).sum() / np.abs(r64).sum())
+        out_fp64 = {"value": v64, "unit": UNIT, "ms_per_step": res[m.F64]["ms"] / a.steps,
+                    "sweep_ms": list(res[m.F64]["sweeps_ms"]),
+                    "hbm_frac_step": cells * 2 * BYTES_PER_CELL_SWEEP[8] / (res[m.F64]["ms"] / a.steps / 1e3) / 1e9
+                    / peaks()[0]}
+
+    # roofline of the dominant FP32 kernel (the slower sweep)
+    hbm, kind = peaks()
+    mx, my = res[m.F32]["sweeps_ms"]
+    dom, dom_ms = ("sweep_y", my) if my >= mx else ("sweep_x", mx)
+    alg = cells * BYTES_PER_CELL_SWEEP[4]
+    achieved = alg / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f).get(f"fp32_{dom}")
+        if tj:
+            traffic = tj["bytes_per_cell"] * cells
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic, "kernel": dom, "kernel_ms": dom_ms, "algorithmic_bytes": alg,
+                "peak_kind": kind, "sweep_ms": [mx, my]}
+
+    # e2e through the C ABI with pinned FP64 host buffers
+    e2e = None
+    if rank == 0 or True:
+        U = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
+        T = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
+        ws = m.GpuWorkspace()
+        m.init_gpu_workspace(ws, U)
+        m.set_gpu_physics_gamma(ws, cfg.gamma)
+        ws.set_limiter(limiter)
+        ws.set_stream(stream.cuda_stream)
+        hin = torch.from_numpy(U0).pin_memory()
+        hout = torch.empty_like(hin).pin_memory()
+        a_in, a_out = hin.numpy(), hout.numpy()
+        for _ in range(2):  # warm-up
+            ws.upload(U, a_in)
+            ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
+            ws.download(U, a_out)
+        ws.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.e2e_steps):
+            ws.upload(U, a_in)
+            ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
+            ws.download(U, a_out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        ws.destroy()
+        nbytes = U0.nbytes
+        e2e = {"value": world * cells * a.e2e_steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": a.e2e_steps,
+               "what": "per step: H2D of the FP64 SoA state from pinned memory, one FP32-bulk step, D2H of the state"}
+
+    cpu = None
+    if world == 1 and rank == 0 and not a.no_cpu_baseline:
+        secs, threads, err = cpu_reference_run(n, 1000, 0, a.cpu_seconds)
+        if err is None:
+            cpu = {"value": cells * len(secs) / sum(secs), "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"reference CPU/OpenMP step (oracle/_ref), Orszag-Tang {n}x{n}, HLLD, minmod "
+                             f"(no van Leer in the reference), {len(secs)} steps after one probe step, FP64"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": err}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": res[m.F32]["ms"] / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (deterministic Orszag-Tang initial data)",
+            "config": {"workload": f"orszag_tang_unit_{n}x{n}_hlld_vanleer_cfl0.4", "nx": n, "ny": n,
+                       "solver": "hlld", "limiter": "vanleer", "precision": "fp32-bulk (fp64 low-beta pressure, "
+                       "fp64 dt reduction)", "per_gpu": "one independent instance",
+                       "l2": "state 604 MB (fp32) / 1.2 GB (fp64) > 126 MB L2; no flush"},
+            "fp64": out_fp64,
+            "fp32_over_fp64": (v32 / out_fp64["value"]) if out_fp64 else None,
+            "rho_rel_l1_fp32_vs_fp64": l1,
+            "hbm_frac_step": cells * 2 * BYTES_PER_CELL_SWEEP[4] / (res[m.F32]["ms"] / a.steps / 1e3) / 1e9 / hbm,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": res[m.F32]["launches"],
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    world, rank, local = dist_setup()
+    if a.impl == "reference":
+        return run_reference_arm(a, world, rank)
+    return run_ours(a, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,185 @@
+/*
+ * mhd_b200.h -- C ABI of the B200-native 2D Dedner GLM-MHD step.
+ *
+ * This is the drop-in boundary for the reference's src/gpu path
+ * (HarryKKKKK/MHD_gpu_acc).  Every entry point takes plain pointers, sizes
+ * and scalars; none exits the process.  Each returns MHD_OK (0) or a negative
+ * MHD_ERR_* code; mhd_last_error() returns a message for the calling thread.
+ * The C++ drop-in headers under include/mhd_b200/ (types.hpp, riemann.hpp,
+ * test_cases.hpp, gpu/grid_gpu.cuh, gpu/solver_gpu.cuh, gpu/boundary_gpu.cuh)
+ * implement the reference's C++ API on top of these functions.
+ *
+ * Device state layout ("grid"): one allocation holding 9 SoA planes in the
+ * field order of the reference's Conserved (head/types.hpp:16-41):
+ * rho, rhou, rhov, rhow, Bx, By, Bz, E, psi.  Cell (i, j) -- ghosts included,
+ * as in Grid2DGPUView::flat_index (head/gpu/grid_gpu.cuh:314-316) -- of field f
+ * is element  f*plane + j*pitch + i.  mhd_grid_alloc pads pitch and plane to
+ * 256 bytes.  Host arrays exchanged with upload/download are dense FP64 SoA of
+ * shape (9, ny+2ng, nx+2ng) (or the reference's AoS Conserved array for the
+ * *_aos variants).
+ */
+#ifndef MHD_B200_H
+#define MHD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MHD_NV 9
+#define MHD_MAX_NG 4
+
+/* ---- error codes ---- */
+#define MHD_OK 0
+#define MHD_ERR_ARG (-1)       /* invalid argument / size / layout */
+#define MHD_ERR_CUDA (-2)      /* a CUDA runtime call failed */
+#define MHD_ERR_NO_SPEED (-3)  /* max wave speed <= 0 (the reference throws: src/cpu/solver_cpu.cpp:304-306) */
+#define MHD_ERR_BAD_DT (-4)    /* dt non-finite or <= 0 (scripts/gpu/main_gpu.cu:219-223) */
+#define MHD_ERR_TINY_DT (-5)   /* dt < 1e-8 t_end (scripts/gpu/main_gpu.cu:224-232) */
+#define MHD_ERR_STATE (-6)     /* workspace not initialised / mismatched (src/gpu/solver_gpu.cu:579-580, 626-627) */
+#define MHD_ERR_NOMEM (-7)     /* device or host allocation failed */
+#define MHD_ERR_TIMEOUT (-8)   /* a bounded device wait gave up */
+
+/* ---- enumerations: values equal the reference's enums ---- */
+/* RiemannSolver, head/riemann.hpp:23 */
+#define MHD_HLL 0
+#define MHD_HLLC 1
+#define MHD_HLLD 2
+#define MHD_FORCE 3
+/* BoundaryType, head/test_cases.hpp:11-16 */
+#define MHD_BC_PERIODIC 0
+#define MHD_BC_TRANSMISSIVE 1
+#define MHD_BC_REFLECTING 2
+#define MHD_BC_DIRICHLET 3
+/* slope limiter: minmod is the reference's (src/cpu/solver_cpu.cpp:26-43); van Leer is new */
+#define MHD_LIMITER_MINMOD 0
+#define MHD_LIMITER_VANLEER 1
+/* storage / arithmetic precision */
+#define MHD_F64 0 /* the plain step: matches the reference CPU FP64 path */
+#define MHD_F32 1 /* FP32-bulk step with the flagged FP64 pressure recovery */
+/* CaseId, head/test_cases.hpp:28-33, plus the configurations this build adds */
+#define MHD_CASE_KELVIN_HELMHOLTZ 0
+#define MHD_CASE_SHOCK_BUBBLE 1
+#define MHD_CASE_BRIO_WU 2
+#define MHD_CASE_ORSZAG_TANG 3
+#define MHD_CASE_ORSZAG_TANG_UNIT 4   /* Orszag-Tang on periodic [0,1]^2, rho = 25/(36 pi), p = 5/(12 pi) */
+#define MHD_CASE_SHOCK_BUBBLE_MHD 5   /* Mach-10 MHD shock - dense bubble on [0,1]^2, gamma 5/3 */
+#define MHD_CASE_BRIO_WU_CFL08 6      /* Brio-Wu 800x4, CFL 0.8, all transmissive */
+
+/* ---- device grid (Grid2DGPU / Grid2DGPUView, head/gpu/grid_gpu.cuh:17-277) ---- */
+typedef struct mhd_grid {
+    void* data;       /* device pointer to field 0, cell (0, 0) */
+    long long pitch;  /* elements per row, >= nx + 2 ng */
+    long long plane;  /* elements per field plane, >= pitch * (ny + 2 ng) */
+    int nx, ny, ng;   /* interior cells and ghost layers (2 <= ng <= MHD_MAX_NG) */
+    int dtype;        /* MHD_F64 or MHD_F32 */
+    double x_min, x_max, y_min, y_max;  /* dx = (x_max - x_min) / nx, dy likewise */
+} mhd_grid;
+
+/* Replaces Grid2DGPU::allocate (head/gpu/grid_gpu.cuh:39-58): one padded slab. */
+int mhd_grid_alloc(mhd_grid* g, int nx, int ny, int ng, int dtype, double x_min, double x_max, double y_min,
+                   double y_max);
+/* Replaces Grid2DGPU::release (head/gpu/grid_gpu.cuh:60-77). */
+int mhd_grid_free(mhd_grid* g);
+/* Replaces Grid2DGPU::upload_from_aos / download_to_aos (head/gpu/grid_gpu.cuh:120-177),
+ * synchronous.  `host` is dense FP64 SoA (9, ny+2ng, nx+2ng); FP32 grids convert on the device. */
+int mhd_grid_upload(const mhd_grid* g, const double* host);
+int mhd_grid_download(const mhd_grid* g, double* host);
+/* Same with the reference's AoS Conserved array (9 doubles per cell, row-major). */
+int mhd_grid_upload_aos(const mhd_grid* g, const double* host_aos);
+int mhd_grid_download_aos(const mhd_grid* g, double* host_aos);
+/* Replaces Grid2DGPU::swap (head/gpu/grid_gpu.cuh:179-189). */
+int mhd_grid_swap(mhd_grid* a, mhd_grid* b);
+
+/* ---- workspace (GpuWorkspace, head/gpu/solver_gpu.cuh:9-19) ---- */
+typedef struct mhd_workspace mhd_workspace;
+
+/* Replaces init_gpu_workspace (src/gpu/solver_gpu.cu:549-566). */
+int mhd_workspace_create(const mhd_grid* g, mhd_workspace** ws);
+/* Replaces free_gpu_workspace (src/gpu/solver_gpu.cu:568-573). */
+int mhd_workspace_destroy(mhd_workspace* ws);
+/* All work of this workspace is queued on `stream` (a cudaStream_t; NULL = legacy default). */
+int mhd_workspace_set_stream(mhd_workspace* ws, void* stream);
+/* Replaces set_gpu_physics_gamma (src/gpu/solver_gpu.cu:536-539); per workspace, not process-global. */
+int mhd_set_gamma(mhd_workspace* ws, double gamma);
+/* Replaces set_gpu_physics_ch (src/gpu/solver_gpu.cu:541-544). */
+int mhd_set_ch(mhd_workspace* ws, double ch);
+int mhd_get_ch(const mhd_workspace* ws, double* ch);
+/* Slope limiter for later steps (default minmod, as the reference). */
+int mhd_set_limiter(mhd_workspace* ws, int limiter);
+/* GLM damping ratio c_r = c_p^2 / c_h (default 0.18, head/physics.hpp:39). */
+int mhd_set_cr(mhd_workspace* ws, double cr);
+
+/* Replaces compute_dt_gpu (src/gpu/solver_gpu.cu:578-605): CFL maximum over the
+ * interior floored by the current ch; sets ch to it and returns
+ * dt = cfl * min(dx, dy) / max.  Returns MHD_ERR_NO_SPEED where the reference
+ * CPU path throws (the reference GPU returned DBL_MAX there); *dt is then DBL_MAX. */
+int mhd_compute_dt(mhd_workspace* ws, const mhd_grid* g, double cfl, double* dt);
+
+/* Replaces advance_second_order_gpu (src/gpu/solver_gpu.cu:617-690): x-sweep
+ * Uold -> Utmp, boundary conditions, y-sweep Utmp -> Unew, boundary conditions,
+ * psi damping -- one fused kernel per sweep.  bc = {left, right, bottom, top}. */
+int mhd_advance(mhd_workspace* ws, const mhd_grid* Uold, mhd_grid* Utmp, mhd_grid* Unew, double dt, int solver,
+                const int* bc);
+
+/* Replaces apply_boundary_gpu (src/gpu/boundary_gpu.cu:158-176), in place. */
+int mhd_apply_boundary(mhd_workspace* ws, mhd_grid* g, const int* bc);
+
+/* ---- device-resident run: the driver loop of scripts/gpu/main_gpu.cu:208-264 ----
+ * The time step, its clamp to t_end and the dt guards are evaluated on the GPU
+ * (the CFL maximum is folded into the y-sweep), and the step loop is captured
+ * once as a CUDA graph of two steps.  U holds the state on entry and exit; T is
+ * the intermediate (x-swept) state.  Stops after max_steps steps (if > 0) or at
+ * t_end, whichever comes first. */
+typedef struct mhd_run_info {
+    double t;          /* simulated time reached */
+    double last_dt;    /* dt of the last step taken */
+    double ch;         /* ch_glm after the last step */
+    int steps;         /* steps taken */
+    int status;        /* MHD_OK, or MHD_ERR_NO_SPEED / _BAD_DT / _TINY_DT (the step loop stopped) */
+    unsigned int fallbacks;  /* cells reverted by the non-finite update guard */
+    unsigned int pad_;
+} mhd_run_info;
+int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_end, int max_steps, int solver,
+            const int* bc, mhd_run_info* info);
+
+/* Measurement aid (no reference counterpart): advances U by nrep device-clock
+ * steps like mhd_run, launching each sweep separately between CUDA events on the
+ * workspace stream; ms_out[0] / ms_out[1] receive the mean x- / y-sweep kernel
+ * time in milliseconds. */
+int mhd_profile_sweeps(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_end, int solver,
+                       const int* bc, int nrep, float* ms_out);
+
+/* Asynchronous host <-> device copies through the workspace's stream and staging
+ * buffer (pinned host memory gives full bandwidth).  Same layout as mhd_grid_upload. */
+int mhd_upload(mhd_workspace* ws, const mhd_grid* g, const double* host);
+int mhd_download(mhd_workspace* ws, const mhd_grid* g, double* host);
+int mhd_synchronize(mhd_workspace* ws);
+
+/* FP64 diagnostics of a state: out[0] = sum rho dA, out[1] = sum E dA,
+ * out[2] = sum |div B| dA (central differences), out[3] = max |div B|,
+ * out[4] = min rho, out[5] = min p.  Deterministic reduction order. */
+int mhd_diagnostics(mhd_workspace* ws, const mhd_grid* g, double* out6);
+
+/* ---- test cases and initial data (head/test_cases.hpp, head/init.hpp) ---- */
+/* get_n_case_config (src/test_cases.cpp:275-282) for case_id, scale n.
+ * out14: nx, ny, ng, x_min, x_max, y_min, y_max, cfl, t_end, gamma, bc[4]. */
+int mhd_case_config(int case_id, int n, double* out14);
+/* initial_state_at (src/test_cases.cpp:288-296): 9 conserved values at (x, y). */
+int mhd_initial_state(int case_id, double x, double y, double* out9);
+/* initialise_grid (src/init.cpp:34-43): evaluates the initial state at every
+ * cell centre, ghosts included, into dense host SoA (9, ny+2ng, nx+2ng). */
+int mhd_initialise(int case_id, int nx, int ny, int ng, double x_min, double x_max, double y_min, double y_max,
+                   double* host);
+
+/* ---- misc ---- */
+const char* mhd_last_error(void);
+/* Library version string. */
+const char* mhd_version(void);
+/* Number of device kernel launches issued by this library in this process. */
+unsigned long long mhd_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MHD_B200_H */

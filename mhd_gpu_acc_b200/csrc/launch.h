@@ -1,0 +1,44 @@
+// launch.h -- host-side entry points of the kernel translation units.  Only
+// the C-ABI layer (capi.cu) includes this; it is not part of the public API.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "mhd_common.cuh"
+
+namespace mhd {
+
+// One split step Uin -> Utmp (x) -> Uout (y), reference semantics.
+// which: 1 = x-sweep only, 2 = y-sweep only, 3 = both.
+cudaError_t launch_step_f64(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
+                            cudaStream_t st, int yseg, int which = 3);
+cudaError_t launch_step_f32(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
+                            cudaStream_t st, int yseg, int which = 3);
+
+// CFL maximum (floored by ch) folded into *out with atomicMax on the bits.
+cudaError_t launch_max_speed_f64(const DevGrid& g, double gamma, double ch, unsigned long long* out,
+                                 cudaStream_t st, int nsm);
+cudaError_t launch_max_speed_f32(const DevGrid& g, double gamma, double ch, unsigned long long* out,
+                                 cudaStream_t st, int nsm);
+
+// In-place apply_boundary (head/cpu/boundary_cpu.hpp:45-149), any precision.
+cudaError_t launch_apply_boundary(const DevGrid& g, int elem_bytes, const int* bc, cudaStream_t st);
+
+// f64 <-> f32 plane conversion over the whole padded slab.
+cudaError_t launch_convert_f64_to_f32(const DevGrid& src, const DevGrid& dst, cudaStream_t st);
+cudaError_t launch_convert_f32_to_f64(const DevGrid& src, const DevGrid& dst, cudaStream_t st);
+
+// Dense AoS Conserved array (device) <-> grid of either precision.
+cudaError_t launch_aos_to_grid(const double* aos, const DevGrid& dst, int elem_bytes, cudaStream_t st);
+cudaError_t launch_grid_to_aos(const DevGrid& src, int elem_bytes, double* aos, cudaStream_t st);
+
+// FP64 diagnostics: out[0] = sum rho dA, out[1] = sum E dA, out[2] = sum |divB| dA,
+// out[3] = max |divB|, out[4] = min rho, out[5] = min p.  Deterministic
+// (fixed-order) two-pass reduction through `scratch` (>= 6 * 1024 doubles).
+cudaError_t launch_diagnostics(const DevGrid& g, int elem_bytes, double gamma, double dx, double dy,
+                               double* scratch, double* out, cudaStream_t st);
+
+// Clock initialisation: maxbits[0] = bits(max0), maxbits[1] = 0, t = 0, steps = 0.
+cudaError_t launch_clock_init(DevClock* c, const unsigned long long* max0, cudaStream_t st);
+
+}  // namespace mhd

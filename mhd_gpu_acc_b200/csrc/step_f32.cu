@@ -1,0 +1,46 @@
+// step_f32.cu -- the FP32-bulk GLM-MHD step: FP32 storage and arithmetic with
+// the flagged FP64 pressure recovery (phys_fast.cuh), FP64 time step and CFL
+// reduction, driven by the same fused sweeps as the FP64 step (sweep.cuh).
+//
+// Build this translation unit with --use_fast_math.
+#include "launch.h"
+#include "phys_fast.cuh"
+#include "dispatch.cuh"
+
+namespace mhd {
+
+template <int SOLVER, int LIMITER>
+struct FastPolicy {
+    using Real = float;
+    static constexpr int NW = NV;
+    static constexpr int NS = 2 * NV;
+    struct Prim { float v[NV]; };
+    using Side = fast::Side;
+
+    __device__ static void prim(const float* U, double g, float* W) { fast::c2p(U, (float)g, W); }
+
+    template <int DIR>
+    __device__ static void recon(const Prim& Wm, const Prim& Wc, const Prim& Wp, double dtd, double ch, double g,
+                                 Side& L, Side& R) {
+        fast::reconstruct<DIR, LIMITER>(Wm.v, Wc.v, Wp.v, (float)dtd, (float)ch, (float)g, L, R);
+    }
+
+    template <int DIR>
+    __device__ static void face(const Side& Rl, const Side& Lr, double ch, double g, float* F) {
+        fast::riemann<DIR, SOLVER>(Rl, Lr, (float)ch, (float)g, F);
+    }
+
+    __device__ static double speed(const float* U, double g, double ch) { return fast::cell_speed(U, (float)g, ch); }
+};
+
+cudaError_t launch_step_f32(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
+                            cudaStream_t st, int yseg, int which) {
+    return dispatch_step<FastPolicy>(in, tmp, out, P, st, yseg, which);
+}
+
+cudaError_t launch_max_speed_f32(const DevGrid& g, double gamma, double ch, unsigned long long* out,
+                                 cudaStream_t st, int nsm) {
+    return launch_max_policy<FastPolicy<HLL, MINMOD>>(g, gamma, ch, out, st, nsm);
+}
+
+}  // namespace mhd

@@ -1,0 +1,47 @@
+// step_f64.cu -- the FP64 ("plain") GLM-MHD step: the reference-faithful
+// physics of phys_exact.cuh driven by the fused sweeps of sweep.cuh.
+//
+// Build this translation unit with --fmad=false: together with the reference
+// operand order in phys_exact.cuh it makes the GPU step reproduce the
+// reference's CPU/OpenMP FP64 step (src/cpu/solver_cpu.cpp) bit for bit.
+#include "launch.h"
+#include "phys_exact.cuh"
+#include "dispatch.cuh"
+
+namespace mhd {
+
+template <int SOLVER, int LIMITER>
+struct ExactPolicy {
+    using Real = double;
+    static constexpr int NW = NV;  // primitive values per cell
+    static constexpr int NS = NV;  // values per reconstructed side state (U*)
+    struct Prim { double v[NV]; };
+    struct Side { double v[NV]; };
+
+    __device__ static void prim(const double* U, double g, double* W) { exact::c2p(U, g, W); }
+
+    template <int DIR>
+    __device__ static void recon(const Prim& Wm, const Prim& Wc, const Prim& Wp, double dtd, double ch, double g,
+                                 Side& L, Side& R) {
+        exact::reconstruct<DIR, LIMITER>(Wm.v, Wc.v, Wp.v, dtd, ch, g, L.v, R.v);
+    }
+
+    template <int DIR>
+    __device__ static void face(const Side& Rl, const Side& Lr, double ch, double g, double* F) {
+        exact::riemann<DIR, SOLVER>(Rl.v, Lr.v, ch, g, F);
+    }
+
+    __device__ static double speed(const double* U, double g, double ch) { return exact::cell_speed(U, g, ch); }
+};
+
+cudaError_t launch_step_f64(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
+                            cudaStream_t st, int yseg, int which) {
+    return dispatch_step<ExactPolicy>(in, tmp, out, P, st, yseg, which);
+}
+
+cudaError_t launch_max_speed_f64(const DevGrid& g, double gamma, double ch, unsigned long long* out,
+                                 cudaStream_t st, int nsm) {
+    return launch_max_policy<ExactPolicy<HLL, MINMOD>>(g, gamma, ch, out, st, nsm);
+}
+
+}  // namespace mhd
