@@ -124,6 +124,23 @@ int mhd_advance(mhd_workspace* ws, const mhd_grid* Uold, mhd_grid* Utmp, mhd_gri
 /* Replaces apply_boundary_gpu (src/gpu/boundary_gpu.cu:158-176), in place. */
 int mhd_apply_boundary(mhd_workspace* ws, mhd_grid* g, const int* bc);
 
+/* One split step (as mhd_advance) that allocates no device memory.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc -- an
+ * application whose own pool allocator owns all device memory, or a loop that
+ * cannot absorb the synchronisation an allocation may imply -- and therefore
+ * cannot create a workspace or an intermediate state: the x-swept state lives
+ * in a fixed 32 MiB device array inside the library (held by every GPU that
+ * loads it, until exit).  Grids whose intermediate state would not fit
+ * (9 planes of pitch x (ny+2ng) elements, pitch = nx+2ng rounded up to 256
+ * bytes) are rejected with MHD_ERR_ARG.  The array's device address is looked
+ * up on the first call on each device (make that call before any stream
+ * capture).  All calls share the array: calls that can overlap on the GPU race
+ * and must be serialised by the caller.  gamma, ch and cr are the values a
+ * workspace would hold; `stream` is a cudaStream_t (NULL = legacy default). */
+#define MHD_NOALLOC_SCRATCH_BYTES (32u << 20)
+int mhd_advance_noalloc(const mhd_grid* Uold, mhd_grid* Unew, double gamma, double ch, double cr, double dt,
+                        int solver, int limiter, const int* bc, void* stream);
+
 /* ---- device-resident run: the driver loop of scripts/gpu/main_gpu.cu:208-264 ----
  * The time step, its clamp to t_end and the dt guards are evaluated on the GPU
  * (the CFL maximum is folded into the y-sweep), and the step loop is captured

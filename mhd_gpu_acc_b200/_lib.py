@@ -77,6 +77,7 @@ PROTOTYPES = {
     "mhd_compute_dt": (_I, [_P, _pg, _D, _pd]),
     "mhd_advance": (_I, [_P, _pg, _pg, _pg, _D, _I, _pi]),
     "mhd_apply_boundary": (_I, [_P, _pg, _pi]),
+    "mhd_advance_noalloc": (_I, [_pg, _pg, _D, _D, _D, _D, _I, _I, _pi, _P]),
     "mhd_run": (_I, [_P, _pg, _pg, _D, _D, _I, _I, _pi, C.POINTER(mhd_run_info)]),
     "mhd_profile_sweeps": (_I, [_P, _pg, _pg, _D, _D, _I, _pi, _I, C.POINTER(C.c_float)]),
     "mhd_upload": (_I, [_P, _pg, _P]),

@@ -31,6 +31,7 @@ CU_SOURCES = {
     "step_f32.cu": ["--use_fast_math"],
     "aux_kernels.cu": [],
     "capi.cu": [],
+    "noalloc.cu": [],
 }
 CXX_SOURCES = {"cases.cpp": []}
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []

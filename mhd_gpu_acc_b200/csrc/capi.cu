@@ -83,6 +83,14 @@ double gdy(const mhd_grid* g) { return (g->y_max - g->y_min) / static_cast<doubl
 
 }  // namespace
 
+namespace mhd {
+// Lets other translation units of the library report through mhd_last_error().
+int report_error(int code, const char* msg) {
+    g_err = msg;
+    return code;
+}
+}  // namespace mhd
+
 struct mhd_workspace {
     int nx = 0, ny = 0, ng = 0, dtype = 0;
     double gamma = 5.0 / 3.0;  // head/physics.hpp:28 default
