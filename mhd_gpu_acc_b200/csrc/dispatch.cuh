@@ -11,7 +11,8 @@ template <class PH>
 cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
                           cudaStream_t st, int yseg, int which) {
     if (which & 1) {
-        const dim3 bx(32 * XS_ROWS), gx((in.nx + XS_TX - 1) / XS_TX, (in.ny + XS_ROWS - 1) / XS_ROWS);
+        const int rows_per_cta = XS_ROWS * XS_RPW;
+        const dim3 bx(32 * XS_ROWS), gx((in.nx + XS_TX - 1) / XS_TX, (in.ny + rows_per_cta - 1) / rows_per_cta);
         sweep_x_kernel<PH><<<gx, bx, 0, st>>>(in, tmp, P);
     }
     if (which & 2) {

@@ -24,6 +24,16 @@ constexpr float kPFloor = 1.0e-12f;    // src/cpu/solver_cpu.cpp:20
 // Internal energy below this fraction of E takes the FP64 pressure branch.
 constexpr float kLowBetaFrac = 0.02f;
 
+// x * 0 is 0 for finite x and NaN for an infinity or a NaN, so an FMA chain of
+// the values times zero tells whether all are finite with FMA-pipe work and a
+// single comparison (instead of one ALU test per value).
+__device__ __forceinline__ bool all_finite(const float* v, int n) {
+    float z = v[0] * 0.0f;
+    for (int k = 1; k < n; ++k) z = fmaf(v[k], 0.0f, z);
+    return z == 0.0f;
+}
+__device__ __forceinline__ bool both_finite(float a, float b) { return fmaf(a, 0.0f, b * 0.0f) == 0.0f; }
+
 struct Side {
     float v[2 * NV];  // [0, 9): U, [9, 18): W
     __device__ __forceinline__ float* U() { return v; }
@@ -101,7 +111,7 @@ __device__ __forceinline__ float fast_speed(const float* W, float g) {
 }
 
 __device__ __forceinline__ bool riemann_physical(const float* W) {
-    return isfinite(W[RHO]) && isfinite(W[PP]) && W[RHO] > 0.0f && W[PP] > 0.0f;
+    return both_finite(W[RHO], W[PP]) && W[RHO] > 0.0f && W[PP] > 0.0f;
 }
 
 template <int DIR>
@@ -186,7 +196,7 @@ __device__ __forceinline__ void hllc(const Side& L, const Side& R, float ch, flo
     const float SM = numerSM / denomSM;
     const float rhoLs = rhoL * (SL - unL) / (SL - SM);
     const float rhoRs = rhoR * (SR - unR) / (SR - SM);
-    if (rhoLs <= 0.0f || rhoRs <= 0.0f || !isfinite(rhoLs) || !isfinite(rhoRs)) { hll<DIR>(L, R, ch, g, F); return; }
+    if (rhoLs <= 0.0f || rhoRs <= 0.0f || !both_finite(rhoLs, rhoRs)) { hll<DIR>(L, R, ch, g, F); return; }
     const float psiM = 0.5f * (VL[PSI] + VR[PSI]) - 0.5f * ch * (BnR - BnL);
     float Us[NV], Fs[NV];
     if (SM >= 0.0f) {
@@ -245,7 +255,7 @@ __device__ __forceinline__ void hlld(const Side& L, const Side& R, float ch, flo
     const float SM = numerSM / denomSM;
     const float rhoLs = rhoL * (SL - unL) / (SL - SM);
     const float rhoRs = rhoR * (SR - unR) / (SR - SM);
-    if (rhoLs <= 0.0f || rhoRs <= 0.0f || !isfinite(rhoLs) || !isfinite(rhoRs)) { hll<DIR>(L, R, ch, g, F); return; }
+    if (rhoLs <= 0.0f || rhoRs <= 0.0f || !both_finite(rhoLs, rhoRs)) { hll<DIR>(L, R, ch, g, F); return; }
     if (SL >= 0.0f) { flux<DIR>(L.U(), VL, ch, F); return; }
     if (SR <= 0.0f) { flux<DIR>(R.U(), VR, ch, F); return; }
     const float ptstar = ptL + rhoL * (SL - unL) * (SM - unL);
@@ -353,7 +363,7 @@ __device__ __forceinline__ void riemann(const Side& L, const Side& R, float ch, 
     if (SOLVER == HLLC) hllc<DIR>(L, R, ch, g, F);
     else if (SOLVER == HLLD) hlld<DIR>(L, R, ch, g, F);
     else force<DIR>(L, R, ch, g, F);
-    if (!isfinite(F[RHO]) || !isfinite(F[EN]) || !isfinite(F[BX]) || !isfinite(F[PSI])) {
+    if (!(fmaf(F[RHO], 0.0f, fmaf(F[EN], 0.0f, fmaf(F[BX], 0.0f, F[PSI] * 0.0f))) == 0.0f)) {
         hll<DIR>(L, R, ch, g, F);
         return;
     }
@@ -371,10 +381,7 @@ __device__ __forceinline__ float vanleer(float a, float b) {
 }
 
 __device__ __forceinline__ bool is_physical(const float* V) {
-    bool ok = V[RHO] > kRhoFloor && V[PP] > kPFloor;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) ok = ok && isfinite(V[k]);
-    return ok;
+    return V[RHO] > kRhoFloor && V[PP] > kPFloor && all_finite(V, NV);
 }
 
 // MUSCL-Hancock half step (src/cpu/solver_cpu.cpp:88-119; c_h in the predictor).

@@ -32,6 +32,7 @@ namespace mhd {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int XS_TX = 28;       // interior cells per warp in the x-sweep (32 lanes - 4 halo)
 constexpr int XS_ROWS = 8;      // warps (rows) per x-sweep CTA
+constexpr int XS_RPW = 8;       // rows each x-sweep warp processes (with one-row prefetch)
 constexpr int YS_WARPS = 4;     // warps (row segments) per y-sweep CTA
 
 template <int N, typename T>
@@ -160,6 +161,9 @@ __device__ __forceinline__ bool update_cell(const R* U, const R* Fp, const R* Fm
 // ---------------------------------------------------------------------------
 // x-sweep
 // ---------------------------------------------------------------------------
+// Each warp handles rows  blockIdx.y*XS_ROWS*XS_RPW + warp + k*XS_ROWS  (k <
+// XS_RPW) of one 28-column tile and loads the next row's cells before
+// computing the current one, so the load latency overlaps the arithmetic.
 template <class PH>
 __global__ void __launch_bounds__(32 * XS_ROWS) sweep_x_kernel(DevGrid in, DevGrid out, StepParams P) {
     using R = typename PH::Real;
@@ -173,48 +177,60 @@ __global__ void __launch_bounds__(32 * XS_ROWS) sweep_x_kernel(DevGrid in, DevGr
     if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int row = blockIdx.y * XS_ROWS + warp;
-    if (row >= in.ny) return;  // whole warp: no block-level synchronisation follows
+    const int row0 = blockIdx.y * XS_ROWS * XS_RPW;
+    const int row_end = min(in.ny, row0 + XS_ROWS * XS_RPW);
+    int row = row0 + warp;
+    if (row >= row_end) return;  // whole warp: no block-level synchronisation follows
     const int ng = in.ng, ib = ng, ie = ng + in.nx;
-    const int y = ng + row;
     const int x = ib - 2 + blockIdx.x * XS_TX + lane;
+    const bool xin = x < in.tnx();
     const double g = P.gamma;
     const double dtd = dt / P.dx;
+    const bool do_recon = lane >= 1 && lane <= 30 && x >= ib - 1 && x <= ie;
+    const bool do_face = lane >= 1 && lane <= 29 && x >= ib - 1 && x <= ie - 1;
+    const bool do_update = lane >= 2 && lane <= 29 && x >= ib && x < ie;
 
-    R U[NV], W[NV];
+    R Unext[NV];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) U[k] = R(0);
-    U[RHO] = R(1);
-    if (x < in.tnx()) load_cell(in, x, y, U);
-    PH::prim(U, g, W);
+    for (int k = 0; k < NV; ++k) Unext[k] = R(0);
+    Unext[RHO] = R(1);
+    if (xin) load_cell(in, x, ng + row, Unext);
 
-    typename PH::Side L, Rt;
+#pragma unroll 1
+    for (; row < row_end; row += XS_ROWS) {
+        const int y = ng + row;
+        R U[NV], W[NV];
 #pragma unroll
-    for (int k = 0; k < PH::NS; ++k) { L.v[k] = R(0); Rt.v[k] = R(0); }
-    {
-        typename PH::Prim Wm, Wp;
-        shfl_up_n<PH::NW>(W, Wm.v, 1);
-        shfl_down_n<PH::NW>(W, Wp.v, 1);
-        typename PH::Prim Wc;
+        for (int k = 0; k < NV; ++k) U[k] = Unext[k];
+        if (xin && row + XS_ROWS < row_end) load_cell(in, x, y + XS_ROWS, Unext);  // prefetch
+        PH::prim(U, g, W);
+
+        typename PH::Side L, Rt;
 #pragma unroll
-        for (int k = 0; k < PH::NW; ++k) Wc.v[k] = W[k];
-        if (lane >= 1 && lane <= 30 && x >= ib - 1 && x <= ie)
-            PH::template recon<0>(Wm, Wc, Wp, dtd, ch, g, L, Rt);
-    }
-    typename PH::Side Ln;
-    shfl_down_n<PH::NS>(L.v, Ln.v, 1);
-    R F[NV];
+        for (int k = 0; k < PH::NS; ++k) { L.v[k] = R(0); Rt.v[k] = R(0); }
+        {
+            typename PH::Prim Wm, Wp, Wc;
+            shfl_up_n<PH::NW>(W, Wm.v, 1);
+            shfl_down_n<PH::NW>(W, Wp.v, 1);
 #pragma unroll
-    for (int k = 0; k < NV; ++k) F[k] = R(0);
-    if (lane >= 1 && lane <= 29 && x >= ib - 1 && x <= ie - 1) PH::template face<0>(Rt, Ln, ch, g, F);
-    R Fm[NV];
-    shfl_up_n<NV>(F, Fm, 1);
-    if (lane >= 2 && lane <= 29 && x >= ib && x < ie) {
-        R Un[NV];
-        const bool reverted = update_cell<R>(U, F, Fm, R(dtd), Un);
-        if (reverted && P.clock) atomicAdd(&P.clock->flux_fallbacks, 1u);
-        store_cell(out, x, y, Un);
-        if (near_edge(out, x, y)) scatter_ghosts<R>(out, x, y, Un, P.bc);
+            for (int k = 0; k < PH::NW; ++k) Wc.v[k] = W[k];
+            if (do_recon) PH::template recon<0>(Wm, Wc, Wp, dtd, ch, g, L, Rt);
+        }
+        typename PH::Side Ln;
+        shfl_down_n<PH::NS>(L.v, Ln.v, 1);
+        R F[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) F[k] = R(0);
+        if (do_face) PH::template face<0>(Rt, Ln, ch, g, F);
+        R Fm[NV];
+        shfl_up_n<NV>(F, Fm, 1);
+        if (do_update) {
+            R Un[NV];
+            const bool reverted = update_cell<R>(U, F, Fm, R(dtd), Un);
+            if (reverted && P.clock) atomicAdd(&P.clock->flux_fallbacks, 1u);
+            store_cell(out, x, y, Un);
+            if (near_edge(out, x, y)) scatter_ghosts<R>(out, x, y, Un, P.bc);
+        }
     }
 }
 
@@ -246,21 +262,26 @@ __global__ void __launch_bounds__(32 * YS_WARPS) sweep_y_kernel(DevGrid in, DevG
         typename PH::Prim Wm, Wc, Wp;
         typename PH::Side Rprev, L, Rt;
         R Fprev[NV], F[NV], U[NV];
+        R Unext[NV];
         load_cell(in, x, j0 - 2, U);
+        load_cell(in, x, j0 - 1, Unext);
         PH::prim(U, g, Wm.v);
-        load_cell(in, x, j0 - 1, U);
-        PH::prim(U, g, Wc.v);
+        PH::prim(Unext, g, Wc.v);
+        load_cell(in, x, j0, Unext);
 #pragma unroll 1
         for (int r = j0; r <= j1 + 1; ++r) {
-            load_cell(in, x, r, U);
+#pragma unroll
+            for (int k = 0; k < NV; ++k) U[k] = Unext[k];
+            if (r <= j1) load_cell(in, x, r + 1, Unext);  // prefetch the next row
+            R Uc[NV];
+            if (r >= j0 + 2) load_cell(in, x, r - 2, Uc);  // the row updated below
             PH::prim(U, g, Wp.v);
             PH::template recon<1>(Wm, Wc, Wp, dtd, ch, g, L, Rt);  // cell r-1
             if (r >= j0 + 1) {
                 PH::template face<1>(Rprev, L, ch, g, F);  // face (r-2 | r-1)
                 if (r >= j0 + 2) {
                     const int yc = r - 2;
-                    R Uc[NV], Un[NV];
-                    load_cell(in, x, yc, Uc);
+                    R Un[NV];
                     reverts += update_cell<R>(Uc, F, Fprev, R(dtd), Un) ? 1u : 0u;
                     if (near_edge(out, x, yc)) scatter_ghosts<R>(out, x, yc, Un, P.bc);
                     Un[PSI] = Un[PSI] * R(damp);
