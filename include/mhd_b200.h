@@ -188,6 +188,10 @@ int mhd_initial_state(int case_id, double x, double y, double* out9);
 int mhd_initialise(int case_id, int nx, int ny, int ng, double x_min, double x_max, double y_min, double y_max,
                    double* host);
 
+/* riemann_flux with explicit c_h (head/riemann.hpp:568-592) on one face, on the
+ * host, FP64: the functions the FP64 kernels run.  dir 0 = x, 1 = y. */
+int mhd_riemann_flux(const double* UL, const double* UR, int dir, int solver, double ch, double gamma, double* F);
+
 /* ---- misc ---- */
 const char* mhd_last_error(void);
 /* Library version string. */

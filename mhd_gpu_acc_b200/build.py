@@ -32,6 +32,7 @@ CU_SOURCES = {
     "aux_kernels.cu": [],
     "capi.cu": [],
     "noalloc.cu": [],
+    "compat.cu": ["--fmad=false"],
 }
 CXX_SOURCES = {"cases.cpp": []}
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []
@@ -60,6 +61,8 @@ def _run(cmd: list[str]) -> None:
 def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "mhd_b200.h")]
+    for d, _, files in os.walk(os.path.join(ROOT, "include", "mhd_b200")):
+        hdrs += [os.path.join(d, f) for f in files]
     tasks, objs = [], []
     nv = nvcc()
     for src, flags in CU_SOURCES.items():

@@ -12,11 +12,19 @@
 //                                     src/cpu/solver_cpu.cpp:26-43, 49-70, 88-119
 // Additions without a reference counterpart: the van Leer limiter.
 //
+// The functions are __host__ __device__: the host side of the library uses
+// them for the reference's header-inline API (cons_to_prim, riemann_flux).
 // States are plain double[9] arrays (field order of mhd_common.cuh); the
 // direction is a template parameter so each sweep gets straight-line code.
 #pragma once
 
 #include "mhd_common.cuh"
+
+#ifdef __CUDACC__
+#define MHD_HD_INLINE __host__ __device__ __forceinline__
+#else
+#define MHD_HD_INLINE inline
+#endif
 
 namespace mhd {
 namespace exact {
@@ -24,7 +32,7 @@ namespace exact {
 constexpr double kRhoFloor = 1.0e-12;  // src/cpu/solver_cpu.cpp:19
 constexpr double kPFloor = 1.0e-12;    // src/cpu/solver_cpu.cpp:20
 
-__device__ __forceinline__ void c2p(const double* U, double g, double* W) {
+MHD_HD_INLINE void c2p(const double* U, double g, double* W) {
     const double inv_rho = 1.0 / U[RHO];
     const double ux = U[MX] * inv_rho;
     const double uy = U[MY] * inv_rho;
@@ -36,7 +44,7 @@ __device__ __forceinline__ void c2p(const double* U, double g, double* W) {
     W[BX] = U[BX]; W[BY] = U[BY]; W[BZ] = U[BZ]; W[PP] = p; W[PSI] = U[PSI];
 }
 
-__device__ __forceinline__ void p2c(const double* V, double g, double* U) {
+MHD_HD_INLINE void p2c(const double* V, double g, double* U) {
     const double Bmag2 = V[BX] * V[BX] + V[BY] * V[BY] + V[BZ] * V[BZ];
     const double ke = 0.5 * V[RHO] * (V[PU] * V[PU] + V[PV] * V[PV] + V[PW] * V[PW]);
     const double E = V[PP] / (g - 1.0) + ke + 0.5 * Bmag2;
@@ -45,7 +53,7 @@ __device__ __forceinline__ void p2c(const double* V, double g, double* U) {
 }
 
 template <int DIR>
-__device__ __forceinline__ void flux(const double* U, double ch, double g, double* F) {
+MHD_HD_INLINE void flux(const double* U, double ch, double g, double* F) {
     const double inv_rho = 1.0 / U[RHO];
     const double ux = U[MX] * inv_rho;
     const double uy = U[MY] * inv_rho;
@@ -79,7 +87,7 @@ __device__ __forceinline__ void flux(const double* U, double ch, double g, doubl
 }
 
 template <int DIR>
-__device__ __forceinline__ double fast_speed(const double* V, double g) {
+MHD_HD_INLINE double fast_speed(const double* V, double g) {
     const double a2 = g * V[PP] / V[RHO];
     const double b2 = (V[BX] * V[BX] + V[BY] * V[BY] + V[BZ] * V[BZ]) / V[RHO];
     const double Bn = (DIR == 0) ? V[BX] : V[BY];
@@ -88,19 +96,19 @@ __device__ __forceinline__ double fast_speed(const double* V, double g) {
     return sqrt(0.5 * (a2 + b2 + sqrt(disc > 0.0 ? disc : 0.0)));
 }
 
-__device__ __forceinline__ bool riemann_physical(const double* V) {
+MHD_HD_INLINE bool riemann_physical(const double* V) {
     return isfinite(V[RHO]) && isfinite(V[PP]) && V[RHO] > 0.0 && V[PP] > 0.0;
 }
 
 template <int DIR>
-__device__ __forceinline__ void rotate(const double* V, double& un, double& ut, double& uw, double& Bn,
+MHD_HD_INLINE void rotate(const double* V, double& un, double& ut, double& uw, double& Bn,
                                        double& Bt, double& Bw) {
     if (DIR == 0) { un = V[PU]; ut = V[PV]; uw = V[PW]; Bn = V[BX]; Bt = V[BY]; Bw = V[BZ]; }
     else          { un = V[PV]; ut = V[PU]; uw = V[PW]; Bn = V[BY]; Bt = V[BX]; Bw = V[BZ]; }
 }
 
 template <int DIR>
-__device__ __forceinline__ void build_star(double rhos, double uns, double uts, double uws, double Bns,
+MHD_HD_INLINE void build_star(double rhos, double uns, double uts, double uws, double Bns,
                                            double Bts, double Bws, double Es, double psis, double* U) {
     U[RHO] = rhos;
     if (DIR == 0) {
@@ -114,7 +122,7 @@ __device__ __forceinline__ void build_star(double rhos, double uns, double uts, 
 }
 
 template <int DIR>
-__device__ __forceinline__ void hll(const double* UL, const double* UR, double ch, double g, double* F) {
+MHD_HD_INLINE void hll(const double* UL, const double* UR, double ch, double g, double* F) {
     double VL[NV], VR[NV], FL[NV], FR[NV];
     c2p(UL, g, VL);
     c2p(UR, g, VR);
@@ -155,7 +163,7 @@ __device__ __forceinline__ void hll(const double* UL, const double* UR, double c
 }
 
 template <int DIR>
-__device__ __forceinline__ void hllc(const double* UL, const double* UR, double ch, double g, double* F) {
+MHD_HD_INLINE void hllc(const double* UL, const double* UR, double ch, double g, double* F) {
     double VL[NV], VR[NV];
     c2p(UL, g, VL);
     c2p(UR, g, VR);
@@ -218,7 +226,7 @@ __device__ __forceinline__ void hllc(const double* UL, const double* UR, double 
 }
 
 template <int DIR>
-__device__ __forceinline__ void hlld(const double* UL, const double* UR, double ch, double g, double* F) {
+MHD_HD_INLINE void hlld(const double* UL, const double* UR, double ch, double g, double* F) {
     double VL[NV], VR[NV];
     c2p(UL, g, VL);
     c2p(UR, g, VR);
@@ -376,7 +384,7 @@ __device__ __forceinline__ void hlld(const double* UL, const double* UR, double 
 }
 
 template <int DIR>
-__device__ __forceinline__ void force(const double* UL, const double* UR, double ch, double g, double* F) {
+MHD_HD_INLINE void force(const double* UL, const double* UR, double ch, double g, double* F) {
     double VL[NV], VR[NV], FL[NV], FR[NV];
     c2p(UL, g, VL);
     c2p(UR, g, VR);
@@ -417,7 +425,7 @@ __device__ __forceinline__ void force(const double* UL, const double* UR, double
 }
 
 template <int DIR>
-__device__ __forceinline__ void glm_overwrite(double* F, const double* UL, const double* UR, double ch) {
+MHD_HD_INLINE void glm_overwrite(double* F, const double* UL, const double* UR, double ch) {
     if (ch <= 0.0) return;
     const double BnL = (DIR == 0) ? UL[BX] : UL[BY];
     const double BnR = (DIR == 0) ? UR[BX] : UR[BY];
@@ -429,7 +437,7 @@ __device__ __forceinline__ void glm_overwrite(double* F, const double* UL, const
 }
 
 template <int DIR, int SOLVER>
-__device__ __forceinline__ void riemann(const double* UL, const double* UR, double ch, double g, double* F) {
+MHD_HD_INLINE void riemann(const double* UL, const double* UR, double ch, double g, double* F) {
     if (SOLVER == HLL) { hll<DIR>(UL, UR, ch, g, F); return; }
     if (SOLVER == HLLC) hllc<DIR>(UL, UR, ch, g, F);
     else if (SOLVER == HLLD) hlld<DIR>(UL, UR, ch, g, F);
@@ -445,17 +453,17 @@ __device__ __forceinline__ void riemann(const double* UL, const double* UR, doub
 // MUSCL-Hancock (src/cpu/solver_cpu.cpp)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ double minmod(double a, double b) {
+MHD_HD_INLINE double minmod(double a, double b) {
     if (a * b <= 0.0) return 0.0;
     return (a > 0.0) ? ((b < a) ? b : a) : ((a < b) ? b : a);
 }
 
-__device__ __forceinline__ double vanleer(double a, double b) {
+MHD_HD_INLINE double vanleer(double a, double b) {
     if (a * b <= 0.0) return 0.0;
     return 2.0 * a * b / (a + b);
 }
 
-__device__ __forceinline__ bool is_physical(const double* V) {
+MHD_HD_INLINE bool is_physical(const double* V) {
     return isfinite(V[RHO]) && V[RHO] > kRhoFloor && isfinite(V[PP]) && V[PP] > kPFloor && isfinite(V[PU]) &&
            isfinite(V[PV]) && isfinite(V[PW]) && isfinite(V[BX]) && isfinite(V[BY]) && isfinite(V[BZ]) &&
            isfinite(V[PSI]);
@@ -464,7 +472,7 @@ __device__ __forceinline__ bool is_physical(const double* V) {
 // reconstruct_cell_muscl_hancock (src/cpu/solver_cpu.cpp:88-119): ch enters
 // the predictor flux (the reference's CPU semantics).
 template <int DIR, int LIMITER>
-__device__ __forceinline__ void reconstruct(const double* Wm, const double* Wc, const double* Wp, double dtd,
+MHD_HD_INLINE void reconstruct(const double* Wm, const double* Wc, const double* Wp, double dtd,
                                             double ch, double g, double* Ul_star, double* Ur_star) {
     double Wl[NV], Wr[NV];
 #pragma unroll
@@ -508,7 +516,7 @@ __device__ __forceinline__ void reconstruct(const double* Wm, const double* Wc, 
 
 // Per-cell CFL speed of compute_dt (src/cpu/solver_cpu.cpp:291-300):
 // returns -1 for a cell the reference skips.
-__device__ __forceinline__ double cell_speed(const double* U, double g, double ch) {
+MHD_HD_INLINE double cell_speed(const double* U, double g, double ch) {
     double V[NV];
     c2p(U, g, V);
     if (!isfinite(V[RHO]) || !isfinite(V[PP]) || V[RHO] <= 0.0 || V[PP] <= 0.0) return -1.0;

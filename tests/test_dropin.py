@@ -1,0 +1,93 @@
+"""The drop-in boundary: the reference's C++ API on libmhd_b200.
+
+CPU: the headers under include/mhd_b200/ compile with a plain C++ compiler;
+the host riemann_flux agrees bit for bit with the reference's (golden known
+answers); the reference's own GPU driver (scripts/gpu/main_gpu.cu) compiles
+unmodified against these headers and links to libmhd_b200 (oracle/Makefile
+`dropin`, built where the reference checkout exists).
+
+GPU: that driver binary runs the reference's Brio-Wu case on the B200 and its
+CSV output (the reference's writer: %.8e, top row first) equals, character
+for character, the same files rendered from the oracle's result.
+"""
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from mhd_gpu_acc_b200 import get_n_case_config, initialise, load
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DROPIN = os.path.join(ROOT, "oracle", "_ref", "main_gpu_dropin")
+
+
+def test_headers_compile_with_gxx(tmp_path):
+    src = tmp_path / "use.cpp"
+    src.write_text(
+        '#include "gpu/boundary_gpu.cuh"\n#include "gpu/grid_gpu.cuh"\n#include "gpu/solver_gpu.cuh"\n'
+        '#include "init.hpp"\n#include "physics.hpp"\n#include "riemann.hpp"\n#include "test_cases.hpp"\n'
+        "int main() { Conserved a(1,0,0,0,0,0,0,2,0), b = 0.5 * (a + a) - a / 2.0; (void)b;\n"
+        "  CaseConfig c = get_n_case_config(CaseId::BrioWu, 1); GpuWorkspace ws; (void)c; (void)ws;\n"
+        "  return phys::cons_to_prim(a).p > 0 ? 0 : 1; }\n")
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(inc, "mhd_b200"), "-I", inc, str(src)],
+                   check=True)
+
+
+def test_host_riemann_flux_matches_reference_kats(golden):
+    _, st = golden
+    lib = load()
+    UL, UR, Fw = st["riemann_UL"], st["riemann_UR"], st["riemann_F"]
+    g, ch = float(st["riemann_gamma"]), float(st["riemann_ch"])
+    F = np.zeros(9)
+    for s in range(4):
+        for d in range(2):
+            for k in range(UL.shape[0]):
+                a = np.ascontiguousarray(UL[k]); b = np.ascontiguousarray(UR[k])
+                assert lib.mhd_riemann_flux(a.ctypes.data, b.ctypes.data, d, s, ch, g, F.ctypes.data) == 0
+                np.testing.assert_array_equal(F, Fw[s, d, k], err_msg=f"solver {s} dir {d} face {k}")
+
+
+def test_reference_driver_links_unmodified():
+    if not os.path.isdir("/root/reference/scripts/gpu"):
+        pytest.skip("reference checkout not present")
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "dropin"], check=True)
+    assert os.access(DROPIN, os.X_OK)
+
+
+def _csv_lines(field: np.ndarray) -> str:
+    """scripts/gpu/main_gpu.cu:36-52 writer: rows top first, %.8e, comma separated."""
+    return "".join(",".join("%.8e" % v for v in row) + "\n" for row in field[::-1])
+
+
+@pytest.mark.gpu
+def test_reference_driver_on_b200_matches_oracle_csv(oracle):
+    if not os.access(DROPIN, os.X_OK):
+        pytest.fail("oracle/_ref/main_gpu_dropin was not built (run __graft_entry__.build())")
+    cfg = get_n_case_config(2, 1)  # the reference's Brio-Wu: CFL 0.4, periodic in y, HLLD
+    with tempfile.TemporaryDirectory() as d:
+        r = subprocess.run([DROPIN, "1", "--case", "brio_wu", "--solver", "hlld", "--out", d], capture_output=True,
+                           text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        U0 = initialise(2, cfg.nx, cfg.ny, cfg.ng, cfg.extent)
+        # the GPU driver applies boundary conditions to the initial data (main_gpu.cu:195)
+        U0 = oracle.apply_boundary(U0, cfg.ng, (cfg.bc.left, cfg.bc.right, cfg.bc.bottom, cfg.bc.top))
+        rc, U, t, steps, ch, _ = oracle.run(U0, cfg.ng, cfg.dx, cfg.dy, cfg.gamma, cfg.cfl, 2, 0,
+                                            (cfg.bc.left, cfg.bc.right, cfg.bc.bottom, cfg.bc.top), t_end=cfg.t_end)
+        assert rc == 0 and f"Total steps= {steps}" in r.stdout
+        ng = cfg.ng
+        I = U[:, ng:-ng, ng:-ng]
+        rho, mu, mv, mw, bx, by, bz, E, psi = I
+        inv = 1.0 / rho
+        ux, uy, uz = mu * inv, mv * inv, mw * inv
+        p = (cfg.gamma - 1.0) * (E - 0.5 * rho * (ux * ux + uy * uy + uz * uz) - 0.5 * (bx * bx + by * by + bz * bz))
+        fields = {"rho": rho, "u": mu / rho, "v": mv / rho, "w": mw / rho, "Bx": bx, "By": by, "Bz": bz, "E": E,
+                  "psi": psi, "p": p}
+        for name, arr in fields.items():
+            path = os.path.join(d, f"brio_wu_gpu_t10_{name}.csv")
+            with open(path) as f:
+                got = f.read()
+            assert got == _csv_lines(arr), name
