@@ -192,6 +192,12 @@ int mhd_initialise(int case_id, int nx, int ny, int ng, double x_min, double x_m
  * host, FP64: the functions the FP64 kernels run.  dir 0 = x, 1 = y. */
 int mhd_riemann_flux(const double* UL, const double* UR, int dir, int solver, double ch, double gamma, double* F);
 
+/* Initial data of case_id evaluated on the device at every cell centre of g
+ * (ghosts included), without a host array.  Agrees with mhd_initialise to the
+ * rounding of the device sin/tanh/exp.  ws may be NULL (then synchronous on the
+ * legacy stream). */
+int mhd_initialise_device(mhd_workspace* ws, const mhd_grid* g, int case_id);
+
 /* ---- misc ---- */
 const char* mhd_last_error(void);
 /* Library version string. */

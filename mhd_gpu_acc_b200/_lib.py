@@ -88,6 +88,7 @@ PROTOTYPES = {
     "mhd_initial_state": (_I, [_I, _D, _D, _pd]),
     "mhd_initialise": (_I, [_I, _I, _I, _I, _D, _D, _D, _D, _P]),
     "mhd_riemann_flux": (_I, [_P, _P, _I, _I, _D, _D, _P]),
+    "mhd_initialise_device": (_I, [_P, _pg, _I]),
     "mhd_last_error": (C.c_char_p, []),
     "mhd_version": (C.c_char_p, []),
     "mhd_launch_count": (C.c_ulonglong, []),

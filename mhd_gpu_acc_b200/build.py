@@ -22,6 +22,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libmhd_b200.so")
+DRIVER = os.path.join(PKG, "mhd_run_case")  # the init / step / output driver (csrc/driver.cpp)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
@@ -33,6 +34,7 @@ CU_SOURCES = {
     "capi.cu": [],
     "noalloc.cu": [],
     "compat.cu": ["--fmad=false"],
+    "ic_kernels.cu": ["--fmad=false"],
 }
 CXX_SOURCES = {"cases.cpp": []}
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []
@@ -85,6 +87,10 @@ def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
         list(ex.map(_run, tasks))
     if tasks or force or _stale(LIB, objs):
         _run([nv, "-shared", *ARCH, "-cudart", "static", "-o", LIB, *objs, "-lpthread", "-ldl", "-lrt"])
+    drv_src = os.path.join(CSRC, "driver.cpp")
+    if force or _stale(DRIVER, [drv_src, LIB] + hdrs):
+        _run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), drv_src, "-o", DRIVER, "-L", PKG,
+              "-lmhd_b200", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

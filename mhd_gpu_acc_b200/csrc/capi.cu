@@ -624,6 +624,18 @@ int mhd_download(mhd_workspace* ws, const mhd_grid* g, double* host) {
     return download_impl(g, host, ws->d_stage, ws->stream);
 }
 
+int mhd_initialise_device(mhd_workspace* ws, const mhd_grid* g, int case_id) {
+    int rc = check_grid(g, "mhd_initialise_device");
+    if (rc) return rc;
+    if (case_id < MHD_CASE_KELVIN_HELMHOLTZ || case_id > MHD_CASE_BRIO_WU_CFL08)
+        return fail(MHD_ERR_ARG, "mhd_initialise_device: unknown case %d", case_id);
+    cudaStream_t st = ws ? ws->stream : nullptr;
+    g_launches += 1;
+    CK(mhd::launch_initialise(dev(g), (int)elem_bytes(g->dtype), case_id, g->x_min, g->y_min, gdx(g), gdy(g), st));
+    if (!ws) CK(cudaStreamSynchronize(nullptr));
+    return MHD_OK;
+}
+
 int mhd_synchronize(mhd_workspace* ws) {
     if (!ws) return fail(MHD_ERR_STATE, "mhd_synchronize: null workspace");
     CK(cudaStreamSynchronize(ws->stream));

@@ -38,6 +38,10 @@ cudaError_t launch_grid_to_aos(const DevGrid& src, int elem_bytes, double* aos, 
 cudaError_t launch_diagnostics(const DevGrid& g, int elem_bytes, double gamma, double dx, double dy,
                                double* scratch, double* out, cudaStream_t st);
 
+// Initial data of case `id` evaluated on the device at every cell centre.
+cudaError_t launch_initialise(const DevGrid& g, int elem_bytes, int id, double x0, double y0, double dx, double dy,
+                              cudaStream_t st);
+
 // Clock initialisation: maxbits[0] = bits(max0), maxbits[1] = 0, t = 0, steps = 0.
 cudaError_t launch_clock_init(DevClock* c, const unsigned long long* max0, cudaStream_t st);
 
