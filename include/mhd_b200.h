@@ -198,6 +198,55 @@ int mhd_riemann_flux(const double* UL, const double* UR, int dir, int solver, do
  * legacy stream). */
 int mhd_initialise_device(mhd_workspace* ws, const mhd_grid* g, int case_id);
 
+/* Orszag-Tang on [0,1]^2 with field amplitude b0 (1/sqrt(4 pi) in the standard
+ * case) and adiabatic exponent gamma: rho = 25/(36 pi), p = 5/(12 pi),
+ * v = (-sin 2pi y, sin 2pi x), B = b0 (-sin 2pi y, sin 4pi x), psi = 0, plus,
+ * when amp != NULL (16 values), divergence-free Fourier perturbations:
+ * with theta_j = 2 pi (m_j . x) and the modes m_j = (1,0), (0,1), (1,1),
+ * (1,-1), (2,0), (0,2), (2,1), (1,2) (j = 0..7),
+ *   du = -sum_j amp[j]   sin(theta_j) m_jy/|m_j|,  dv = sum_j amp[j]   sin(theta_j) m_jx/|m_j|,
+ *   dBx = -sum_j amp[8+j] sin(theta_j) m_jy/|m_j|, dBy = sum_j amp[8+j] sin(theta_j) m_jx/|m_j|.
+ * Evaluated on the device at every cell centre of g (ghosts included). */
+int mhd_initialise_orszag_tang(mhd_workspace* ws, const mhd_grid* g, double b0, double gamma, const double* amp);
+
+/* ---- batched instances (no reference counterpart) ----
+ * Many independent problems of uneven size advanced together: one persistent
+ * launch per sweep phase over a global tile work list, CUDA-graph step loop,
+ * per-instance gamma, CFL, c_r, boundary types, t_end, dt and c_h.  Solver,
+ * limiter and precision are shared.  Dirichlet sides are not supported. */
+typedef struct mhd_instance_desc {
+    int nx, ny, ng;
+    int bc[4];
+    double x_min, x_max, y_min, y_max;
+    double gamma, cfl, cr, t_end;
+} mhd_instance_desc;
+/* Launch shape of the batched sweeps: x-sweep rows per warp, y-sweep segment
+ * length, persistent CTAs of each phase (0 = default from the SM count). */
+typedef struct mhd_batch_tuning {
+    int xrpw, yseg, ctas_x, ctas_y;
+} mhd_batch_tuning;
+typedef struct mhd_batch mhd_batch;
+
+int mhd_batch_create(const mhd_instance_desc* desc, int n, int dtype, int solver, int limiter, mhd_batch** out);
+int mhd_batch_destroy(mhd_batch* b);
+int mhd_batch_set_stream(mhd_batch* b, void* stream);
+/* The state grid of instance i (device memory owned by the batch): fill it with
+ * mhd_grid_upload / mhd_initialise_device / mhd_initialise_orszag_tang, read it
+ * with mhd_grid_download. */
+int mhd_batch_grid(const mhd_batch* b, int i, mhd_grid* out);
+/* Total interior cells of all instances. */
+int mhd_batch_cells(const mhd_batch* b, long long* cells);
+/* Advances every instance by max_steps steps (or to its t_end); info (n
+ * entries, may be NULL) receives each instance's t, steps, dt, c_h, status. */
+int mhd_batch_run(mhd_batch* b, int max_steps, mhd_run_info* info);
+int mhd_batch_get_tuning(const mhd_batch* b, mhd_batch_tuning* t);
+int mhd_batch_set_tuning(mhd_batch* b, const mhd_batch_tuning* t);
+/* Autotuner: times each sweep phase for every candidate launch shape (x rows
+ * per warp 2/4/8/16 x 1-2 CTAs per SM; y segment 16/32/64/128 x 2-4 CTAs per
+ * SM) on the batch's current states, `reps` launches each, and keeps the
+ * fastest.  Leaves the instances one step ahead. */
+int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best);
+
 /* ---- misc ---- */
 const char* mhd_last_error(void);
 /* Library version string. */

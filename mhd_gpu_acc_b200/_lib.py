@@ -52,6 +52,27 @@ class mhd_run_info(C.Structure):
     ]
 
 
+class mhd_instance_desc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int),
+        ("ny", C.c_int),
+        ("ng", C.c_int),
+        ("bc", C.c_int * 4),
+        ("x_min", C.c_double),
+        ("x_max", C.c_double),
+        ("y_min", C.c_double),
+        ("y_max", C.c_double),
+        ("gamma", C.c_double),
+        ("cfl", C.c_double),
+        ("cr", C.c_double),
+        ("t_end", C.c_double),
+    ]
+
+
+class mhd_batch_tuning(C.Structure):
+    _fields_ = [("xrpw", C.c_int), ("yseg", C.c_int), ("ctas_x", C.c_int), ("ctas_y", C.c_int)]
+
+
 _D, _I, _P = C.c_double, C.c_int, C.c_void_p
 _pd = C.POINTER(C.c_double)
 _pi = C.POINTER(C.c_int)
@@ -89,6 +110,16 @@ PROTOTYPES = {
     "mhd_initialise": (_I, [_I, _I, _I, _I, _D, _D, _D, _D, _P]),
     "mhd_riemann_flux": (_I, [_P, _P, _I, _I, _D, _D, _P]),
     "mhd_initialise_device": (_I, [_P, _pg, _I]),
+    "mhd_initialise_orszag_tang": (_I, [_P, _pg, _D, _D, _P]),
+    "mhd_batch_create": (_I, [C.POINTER(mhd_instance_desc), _I, _I, _I, _I, C.POINTER(_P)]),
+    "mhd_batch_destroy": (_I, [_P]),
+    "mhd_batch_set_stream": (_I, [_P, _P]),
+    "mhd_batch_grid": (_I, [_P, _I, _pg]),
+    "mhd_batch_cells": (_I, [_P, C.POINTER(C.c_longlong)]),
+    "mhd_batch_run": (_I, [_P, _I, C.POINTER(mhd_run_info)]),
+    "mhd_batch_get_tuning": (_I, [_P, C.POINTER(mhd_batch_tuning)]),
+    "mhd_batch_set_tuning": (_I, [_P, C.POINTER(mhd_batch_tuning)]),
+    "mhd_batch_tune": (_I, [_P, _I, C.POINTER(mhd_batch_tuning)]),
     "mhd_last_error": (C.c_char_p, []),
     "mhd_version": (C.c_char_p, []),
     "mhd_launch_count": (C.c_ulonglong, []),

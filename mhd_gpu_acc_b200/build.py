@@ -35,6 +35,7 @@ CU_SOURCES = {
     "noalloc.cu": [],
     "compat.cu": ["--fmad=false"],
     "ic_kernels.cu": ["--fmad=false"],
+    "batch_api.cu": [],
 }
 CXX_SOURCES = {"cases.cpp": []}
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []

@@ -1,0 +1,101 @@
+// batch.cuh -- many independent instances of uneven size advanced together.
+//
+// Each instance (its own grid, gamma, CFL, c_r, boundary types, t_end and
+// device clock) is cut into the same work units the single-grid sweeps use:
+// x units of 28 columns x (XS_ROWS * rpw) rows, y units of 32 columns x
+// (YS_WARPS * seg) rows.  The units of all instances form one global list
+// (prefix offsets in `first`, split by phase: first[0..n] for x, first[n+1..2n+1]
+// for y).  A persistent launch per sweep phase -- `ctas` CTAs striding over the
+// list -- advances every instance; the kernel boundary between the x and y
+// phases is the only synchronisation a step needs, and a CUDA graph of two
+// steps replays the loop.  Instance k's unit 0 performs the clock duties the
+// single-grid kernels give to CTA (0, 0).
+#pragma once
+
+#include "dispatch.cuh"
+
+namespace mhd {
+
+struct BatchInst {
+    DevGrid U, T;
+    StepParams P;  // physics, boundary types, t_end and clock of this instance
+    int x_tiles, x_rblocks;
+    int y_strips, y_groups;
+};
+
+// largest k in [0, n) with first[k] <= u (first is non-decreasing, first[0] = 0)
+__device__ __forceinline__ int find_instance(const int* first, int n, int u) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(first + mid) <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class PH>
+__global__ void __launch_bounds__(32 * XS_ROWS) batch_x_kernel(const BatchInst* __restrict__ inst,
+                                                              const int* __restrict__ first, int n, int parity,
+                                                              int rpw) {
+    const int total = __ldg(first + n);
+    for (int u = blockIdx.x; u < total; u += gridDim.x) {
+        const int k = find_instance(first, n, u);
+        const int local = u - __ldg(first + k);
+        StepParams P = inst[k].P;
+        P.parity = parity;
+        double dt, ch, damp;
+        if (!step_scalars(P, dt, ch, damp)) {
+            if (local == 0 && threadIdx.x == 0) clock_flag_skip(P);
+            continue;
+        }
+        if (local == 0 && threadIdx.x == 0) P.clock->maxbits[parity ^ 1] = 0ull;
+        const int tiles = inst[k].x_tiles;
+        x_tile<PH>(inst[k].U, inst[k].T, P, dt, ch, local % tiles, local / tiles, rpw);
+    }
+}
+
+template <class PH>
+__global__ void __launch_bounds__(32 * YS_WARPS) batch_y_kernel(const BatchInst* __restrict__ inst,
+                                                               const int* __restrict__ first, int n, int parity,
+                                                               int seg) {
+    const int total = __ldg(first + n);
+    const bool lead = (threadIdx.x == 0 && threadIdx.y == 0);
+    for (int u = blockIdx.x; u < total; u += gridDim.x) {
+        const int k = find_instance(first, n, u);
+        const int local = u - __ldg(first + k);
+        StepParams P = inst[k].P;
+        P.parity = parity;
+        double dt, ch, damp;
+        if (!step_scalars(P, dt, ch, damp)) {
+            if (local == 0 && lead) clock_flag_skip(P);
+            continue;
+        }
+        const int strips = inst[k].y_strips;
+        y_segment<PH>(inst[k].T, inst[k].U, P, dt, ch, damp, local % strips,
+                      (local / strips) * YS_WARPS + threadIdx.y, seg);
+        if (local == 0 && lead) clock_advance(P, dt, ch);
+    }
+}
+
+struct BatchLaunch {
+    const BatchInst* inst;
+    const int* first;
+    int n, parity, which, xrpw, yseg, ctas;
+    cudaStream_t st;
+    template <class PH>
+    cudaError_t run() const {
+        if (which == 1) batch_x_kernel<PH><<<ctas, 32 * XS_ROWS, 0, st>>>(inst, first, n, parity, xrpw);
+        else batch_y_kernel<PH><<<ctas, dim3(32, YS_WARPS), 0, st>>>(inst, first + n + 1, n, parity, yseg);
+        return cudaGetLastError();
+    }
+};
+
+template <template <int, int> class POL>
+cudaError_t dispatch_batch(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,
+                           int limiter, int xrpw, int yseg, int ctas, cudaStream_t st) {
+    BatchLaunch go{inst, first, n, parity, which, xrpw, yseg, ctas, st};
+    return with_policy<POL>(solver, limiter, go);
+}
+
+}  // namespace mhd

@@ -636,6 +636,18 @@ int mhd_initialise_device(mhd_workspace* ws, const mhd_grid* g, int case_id) {
     return MHD_OK;
 }
 
+int mhd_initialise_orszag_tang(mhd_workspace* ws, const mhd_grid* g, double b0, double gamma, const double* amp) {
+    int rc = check_grid(g, "mhd_initialise_orszag_tang");
+    if (rc) return rc;
+    if (!(gamma > 1.0)) return fail(MHD_ERR_ARG, "mhd_initialise_orszag_tang: gamma must exceed 1");
+    cudaStream_t st = ws ? ws->stream : nullptr;
+    g_launches += 1;
+    CK(mhd::launch_initialise_ot(dev(g), (int)elem_bytes(g->dtype), b0, gamma, amp, g->x_min, g->y_min, gdx(g),
+                                 gdy(g), st));
+    if (!ws) CK(cudaStreamSynchronize(nullptr));
+    return MHD_OK;
+}
+
 int mhd_synchronize(mhd_workspace* ws) {
     if (!ws) return fail(MHD_ERR_STATE, "mhd_synchronize: null workspace");
     CK(cudaStreamSynchronize(ws->stream));

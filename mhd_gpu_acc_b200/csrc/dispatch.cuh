@@ -1,6 +1,7 @@
 // dispatch.cuh -- runtime (solver, limiter) -> template instance dispatch and
 // launch geometry of the two sweeps, shared by the FP64 and FP32 translation
-// units.  `which` selects the sweeps: 1 = x only, 2 = y only, 3 = both.
+// units.  `which` selects the sweeps: 1 = x only, 2 = y only, 3 = both;
+// `yseg` is the y-sweep segment length and `xrpw` the x-sweep rows per warp.
 #pragma once
 
 #include "sweep.cuh"
@@ -9,11 +10,11 @@ namespace mhd {
 
 template <class PH>
 cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                          cudaStream_t st, int yseg, int which) {
+                          cudaStream_t st, int yseg, int which, int xrpw) {
     if (which & 1) {
-        const int rows_per_cta = XS_ROWS * XS_RPW;
+        const int rows_per_cta = XS_ROWS * xrpw;
         const dim3 bx(32 * XS_ROWS), gx((in.nx + XS_TX - 1) / XS_TX, (in.ny + rows_per_cta - 1) / rows_per_cta);
-        sweep_x_kernel<PH><<<gx, bx, 0, st>>>(in, tmp, P);
+        sweep_x_kernel<PH><<<gx, bx, 0, st>>>(in, tmp, P, xrpw);
     }
     if (which & 2) {
         const int nseg = (in.ny + yseg - 1) / yseg;
@@ -23,20 +24,36 @@ cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
     return cudaGetLastError();
 }
 
-template <template <int, int> class POL>
-cudaError_t dispatch_step(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                          cudaStream_t st, int yseg, int which) {
-    switch (P.solver * 2 + P.limiter) {
-        case 0: return launch_policy<POL<HLL, MINMOD>>(in, tmp, out, P, st, yseg, which);
-        case 1: return launch_policy<POL<HLL, VANLEER>>(in, tmp, out, P, st, yseg, which);
-        case 2: return launch_policy<POL<HLLC, MINMOD>>(in, tmp, out, P, st, yseg, which);
-        case 3: return launch_policy<POL<HLLC, VANLEER>>(in, tmp, out, P, st, yseg, which);
-        case 4: return launch_policy<POL<HLLD, MINMOD>>(in, tmp, out, P, st, yseg, which);
-        case 5: return launch_policy<POL<HLLD, VANLEER>>(in, tmp, out, P, st, yseg, which);
-        case 6: return launch_policy<POL<FORCE, MINMOD>>(in, tmp, out, P, st, yseg, which);
-        case 7: return launch_policy<POL<FORCE, VANLEER>>(in, tmp, out, P, st, yseg, which);
+// Calls F::template run<POL<S, L>>() for the runtime (solver, limiter) pair.
+template <template <int, int> class POL, class F>
+cudaError_t with_policy(int solver, int limiter, F&& f) {
+    switch (solver * 2 + limiter) {
+        case 0: return f.template run<POL<HLL, MINMOD>>();
+        case 1: return f.template run<POL<HLL, VANLEER>>();
+        case 2: return f.template run<POL<HLLC, MINMOD>>();
+        case 3: return f.template run<POL<HLLC, VANLEER>>();
+        case 4: return f.template run<POL<HLLD, MINMOD>>();
+        case 5: return f.template run<POL<HLLD, VANLEER>>();
+        case 6: return f.template run<POL<FORCE, MINMOD>>();
+        case 7: return f.template run<POL<FORCE, VANLEER>>();
         default: return cudaErrorInvalidValue;
     }
+}
+
+struct StepLaunch {
+    const DevGrid &in, &tmp, &out;
+    const StepParams& P;
+    cudaStream_t st;
+    int yseg, which, xrpw;
+    template <class PH>
+    cudaError_t run() const { return launch_policy<PH>(in, tmp, out, P, st, yseg, which, xrpw); }
+};
+
+template <template <int, int> class POL>
+cudaError_t dispatch_step(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
+                          cudaStream_t st, int yseg, int which, int xrpw) {
+    StepLaunch go{in, tmp, out, P, st, yseg, which, xrpw};
+    return with_policy<POL>(P.solver, P.limiter, go);
 }
 
 template <class PH>

@@ -86,7 +86,62 @@ __global__ void ic_kernel(DevGrid g, int id, double x0, double y0, double dx, do
     }
 }
 
+struct OTParams {
+    double b0, gamma;
+    double amp[16];
+    int has_amp;
+};
+
+// Fourier modes of the perturbations (mhd_initialise_orszag_tang).
+__device__ __constant__ int kModeX[8] = {1, 0, 1, 1, 2, 0, 2, 1};
+__device__ __constant__ int kModeY[8] = {0, 1, 1, -1, 0, 2, 1, 2};
+
+template <typename R>
+__global__ void ot_kernel(DevGrid g, OTParams prm, double x0, double y0, double dx, double dy) {
+    const double PI = 3.14159265358979323846;
+    const int tx = g.tnx(), ty = g.tny();
+    const long long total = (long long)tx * ty;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(k / tx), i = (int)(k - (long long)j * tx);
+        const double x = x0 + ((double)(i - g.ng) + 0.5) * dx;
+        const double y = y0 + ((double)(j - g.ng) + 0.5) * dy;
+        double u = -sin(2.0 * PI * y), v = sin(2.0 * PI * x);
+        double bx = -prm.b0 * sin(2.0 * PI * y), by = prm.b0 * sin(4.0 * PI * x);
+        if (prm.has_amp) {
+            for (int m = 0; m < 8; ++m) {
+                const double mx = kModeX[m], my = kModeY[m];
+                const double s = sin(2.0 * PI * (mx * x + my * y)) / sqrt(mx * mx + my * my);
+                u -= prm.amp[m] * s * my;
+                v += prm.amp[m] * s * mx;
+                bx -= prm.amp[8 + m] * s * my;
+                by += prm.amp[8 + m] * s * mx;
+            }
+        }
+        const C9 c = make_state(25.0 / (36.0 * PI), u, v, 0.0, bx, by, 0.0, 5.0 / (12.0 * PI), prm.gamma);
+        R* b = static_cast<R*>(g.data) + g.idx(i, j);
+#pragma unroll
+        for (int f = 0; f < NV; ++f) b[f * g.plane] = static_cast<R>(c.v[f]);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_initialise_ot(const DevGrid& g, int elem_bytes, double b0, double gamma, const double* amp,
+                                 double x0, double y0, double dx, double dy, cudaStream_t st) {
+    OTParams prm{};
+    prm.b0 = b0;
+    prm.gamma = gamma;
+    prm.has_amp = amp != nullptr;
+    if (amp)
+        for (int k = 0; k < 16; ++k) prm.amp[k] = amp[k];
+    const long long n = (long long)g.tnx() * g.tny();
+    long long blocks = (n + 255) / 256;
+    if (blocks > 65535LL * 8) blocks = 65535LL * 8;
+    if (elem_bytes == 8) ot_kernel<double><<<(unsigned)blocks, 256, 0, st>>>(g, prm, x0, y0, dx, dy);
+    else ot_kernel<float><<<(unsigned)blocks, 256, 0, st>>>(g, prm, x0, y0, dx, dy);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_initialise(const DevGrid& g, int elem_bytes, int id, double x0, double y0, double dx, double dy,
                               cudaStream_t st) {

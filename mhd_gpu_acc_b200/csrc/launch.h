@@ -11,9 +11,17 @@ namespace mhd {
 // One split step Uin -> Utmp (x) -> Uout (y), reference semantics.
 // which: 1 = x-sweep only, 2 = y-sweep only, 3 = both.
 cudaError_t launch_step_f64(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                            cudaStream_t st, int yseg, int which = 3);
+                            cudaStream_t st, int yseg, int which = 3, int xrpw = kDefaultXRpw);
 cudaError_t launch_step_f32(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                            cudaStream_t st, int yseg, int which = 3);
+                            cudaStream_t st, int yseg, int which = 3, int xrpw = kDefaultXRpw);
+
+// Batched instances: one persistent launch per sweep over the global work list
+// (batch.cuh).  which = 1: x-sweeps of every instance, 2: y-sweeps.
+struct BatchInst;
+cudaError_t launch_batch_f64(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,
+                             int limiter, int xrpw, int yseg, int ctas, cudaStream_t st);
+cudaError_t launch_batch_f32(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,
+                             int limiter, int xrpw, int yseg, int ctas, cudaStream_t st);
 
 // CFL maximum (floored by ch) folded into *out with atomicMax on the bits.
 cudaError_t launch_max_speed_f64(const DevGrid& g, double gamma, double ch, unsigned long long* out,
@@ -41,6 +49,10 @@ cudaError_t launch_diagnostics(const DevGrid& g, int elem_bytes, double gamma, d
 // Initial data of case `id` evaluated on the device at every cell centre.
 cudaError_t launch_initialise(const DevGrid& g, int elem_bytes, int id, double x0, double y0, double dx, double dy,
                               cudaStream_t st);
+
+// Parametrised Orszag-Tang initial data (mhd_initialise_orszag_tang).
+cudaError_t launch_initialise_ot(const DevGrid& g, int elem_bytes, double b0, double gamma, const double* amp,
+                                 double x0, double y0, double dx, double dy, cudaStream_t st);
 
 // Clock initialisation: maxbits[0] = bits(max0), maxbits[1] = 0, t = 0, steps = 0.
 cudaError_t launch_clock_init(DevClock* c, const unsigned long long* max0, cudaStream_t st);

@@ -6,6 +6,7 @@
 #include "launch.h"
 #include "phys_fast.cuh"
 #include "dispatch.cuh"
+#include "batch.cuh"
 
 namespace mhd {
 
@@ -34,8 +35,13 @@ struct FastPolicy {
 };
 
 cudaError_t launch_step_f32(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                            cudaStream_t st, int yseg, int which) {
-    return dispatch_step<FastPolicy>(in, tmp, out, P, st, yseg, which);
+                            cudaStream_t st, int yseg, int which, int xrpw) {
+    return dispatch_step<FastPolicy>(in, tmp, out, P, st, yseg, which, xrpw);
+}
+
+cudaError_t launch_batch_f32(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,
+                             int limiter, int xrpw, int yseg, int ctas, cudaStream_t st) {
+    return dispatch_batch<FastPolicy>(inst, first, n, parity, which, solver, limiter, xrpw, yseg, ctas, st);
 }
 
 cudaError_t launch_max_speed_f32(const DevGrid& g, double gamma, double ch, unsigned long long* out,

@@ -32,7 +32,9 @@ namespace mhd {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int XS_TX = 28;       // interior cells per warp in the x-sweep (32 lanes - 4 halo)
 constexpr int XS_ROWS = 8;      // warps (rows) per x-sweep CTA
-constexpr int XS_RPW = 8;       // rows each x-sweep warp processes (with one-row prefetch)
+// rows each x-sweep warp processes (with one-row prefetch) and rows per y-sweep
+// warp segment are launch parameters; their defaults are kDefaultXRpw and
+// kDefaultYSeg (mhd_common.cuh), the autotuner may pick others.
 constexpr int YS_WARPS = 4;     // warps (row segments) per y-sweep CTA
 
 template <int N, typename T>
@@ -161,28 +163,21 @@ __device__ __forceinline__ bool update_cell(const R* U, const R* Fp, const R* Fm
 // ---------------------------------------------------------------------------
 // x-sweep
 // ---------------------------------------------------------------------------
-// Each warp handles rows  blockIdx.y*XS_ROWS*XS_RPW + warp + k*XS_ROWS  (k <
-// XS_RPW) of one 28-column tile and loads the next row's cells before
-// computing the current one, so the load latency overlaps the arithmetic.
+// One CTA of XS_ROWS warps handles a 28-column tile over XS_ROWS * rpw rows:
+// warp w takes rows  row_block*XS_ROWS*rpw + w + k*XS_ROWS  (k < rpw) and loads
+// the next row's cells before computing the current one, so the load latency
+// overlaps the arithmetic.
 template <class PH>
-__global__ void __launch_bounds__(32 * XS_ROWS) sweep_x_kernel(DevGrid in, DevGrid out, StepParams P) {
+__device__ __forceinline__ void x_tile(const DevGrid& in, const DevGrid& out, const StepParams& P, double dt,
+                                       double ch, int tile_x, int row_block, int rpw) {
     using R = typename PH::Real;
-    double dt, ch, damp;
-    const bool first = (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0);
-    if (!step_scalars(P, dt, ch, damp)) {
-        if (first) clock_flag_skip(P);
-        return;
-    }
-    if (first && P.clock) P.clock->maxbits[P.parity ^ 1] = 0ull;
-    if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
-
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int row0 = blockIdx.y * XS_ROWS * XS_RPW;
-    const int row_end = min(in.ny, row0 + XS_ROWS * XS_RPW);
+    const int row0 = row_block * XS_ROWS * rpw;
+    const int row_end = min(in.ny, row0 + XS_ROWS * rpw);
     int row = row0 + warp;
     if (row >= row_end) return;  // whole warp: no block-level synchronisation follows
     const int ng = in.ng, ib = ng, ie = ng + in.nx;
-    const int x = ib - 2 + blockIdx.x * XS_TX + lane;
+    const int x = ib - 2 + tile_x * XS_TX + lane;
     const bool xin = x < in.tnx();
     const double g = P.gamma;
     const double dtd = dt / P.dx;
@@ -234,23 +229,34 @@ __global__ void __launch_bounds__(32 * XS_ROWS) sweep_x_kernel(DevGrid in, DevGr
     }
 }
 
-// ---------------------------------------------------------------------------
-// y-sweep
-// ---------------------------------------------------------------------------
 template <class PH>
-__global__ void __launch_bounds__(32 * YS_WARPS) sweep_y_kernel(DevGrid in, DevGrid out, StepParams P, int seg) {
+__global__ void __launch_bounds__(32 * XS_ROWS) sweep_x_kernel(DevGrid in, DevGrid out, StepParams P, int rpw) {
     using R = typename PH::Real;
     double dt, ch, damp;
-    const bool first = (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0);
+    const bool first = (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0);
     if (!step_scalars(P, dt, ch, damp)) {
         if (first) clock_flag_skip(P);
         return;
     }
+    if (first && P.clock) P.clock->maxbits[P.parity ^ 1] = 0ull;
     if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
+    x_tile<PH>(in, out, P, dt, ch, blockIdx.x, blockIdx.y, rpw);
+}
 
+// ---------------------------------------------------------------------------
+// y-sweep
+// ---------------------------------------------------------------------------
+// One warp marches down rows [j0, j0 + seg) of a 32-column strip (lane = column
+// x = strip*32 + lane), then folds its CFL maximum into one atomic (when
+// P.accumulate) and its revert count into the clock.  Called by whole warps.
+template <class PH>
+__device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out, const StepParams& P, double dt,
+                                          double ch, double damp, int strip, int seg_index, int seg) {
+    using R = typename PH::Real;
+    const int lane = threadIdx.x & 31;
     const int ng = in.ng, ib = ng, ie = ng + in.nx, jb = ng, je = ng + in.ny;
-    const int x = blockIdx.x * 32 + threadIdx.x;
-    const int j0 = jb + (blockIdx.y * YS_WARPS + threadIdx.y) * seg;
+    const int x = strip * 32 + lane;
+    const int j0 = jb + seg_index * seg;
     const int j1 = min(j0 + seg, je);
     const bool active = (x >= ib && x < ie && j0 < je);
     const double g = P.gamma;
@@ -305,21 +311,35 @@ __global__ void __launch_bounds__(32 * YS_WARPS) sweep_y_kernel(DevGrid in, DevG
             const double t = __shfl_xor_sync(FULL, vmax, o);
             vmax = (vmax < t) ? t : vmax;
         }
-        if (threadIdx.x == 0) {
+        if (lane == 0) {
             unsigned long long* tgt = P.clock ? &P.clock->maxbits[P.parity ^ 1] : P.max_out;
             if (tgt) atomic_max_pos(tgt, vmax);
         }
     }
-    if (P.clock) {
-        if (reverts) atomicAdd(&P.clock->flux_fallbacks, reverts);
-        if (first) {
-            DevClock* c = P.clock;
-            c->t[P.parity ^ 1] = c->t[P.parity] + dt;
-            c->steps += 1;
-            c->last_dt = dt;
-            c->last_ch = ch;
-        }
+    if (P.clock && reverts) atomicAdd(&P.clock->flux_fallbacks, reverts);
+}
+
+// Clock advance of a completed device-mode step (one thread per step).
+__device__ __forceinline__ void clock_advance(const StepParams& P, double dt, double ch) {
+    DevClock* c = P.clock;
+    c->t[P.parity ^ 1] = c->t[P.parity] + dt;
+    c->steps += 1;
+    c->last_dt = dt;
+    c->last_ch = ch;
+}
+
+template <class PH>
+__global__ void __launch_bounds__(32 * YS_WARPS) sweep_y_kernel(DevGrid in, DevGrid out, StepParams P, int seg) {
+    using R = typename PH::Real;
+    double dt, ch, damp;
+    const bool first = (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0);
+    if (!step_scalars(P, dt, ch, damp)) {
+        if (first) clock_flag_skip(P);
+        return;
     }
+    if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
+    y_segment<PH>(in, out, P, dt, ch, damp, blockIdx.x, blockIdx.y * YS_WARPS + threadIdx.y, seg);
+    if (P.clock && first) clock_advance(P, dt, ch);
 }
 
 // Standalone CFL maximum over the interior (compute_dt, src/cpu/solver_cpu.cpp:283-303)

@@ -1,0 +1,93 @@
+"""Batched instances against the single-grid device loop.
+
+The batch runs the same per-tile device functions with each instance's own
+parameters and clock, so every instance must equal -- bit for bit -- the same
+problem advanced alone by mhd_run, in FP64 and in FP32-bulk, whatever launch
+shape the autotuner picks."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from mhd_gpu_acc_b200 import F32, F64, GpuWorkspace, Grid2DGPU, init_gpu_workspace, load, set_gpu_physics_gamma
+from mhd_gpu_acc_b200.batch import SQRT_4PI, Batch, instance, orszag_tang_batch_spec
+
+
+def test_batch_spec_is_deterministic():
+    d1, b1, g1 = orszag_tang_batch_spec(3, n=256)
+    d2, b2, g2 = orszag_tang_batch_spec(3, n=256)
+    assert [d.nx for d in d1] == [d.nx for d in d2] and np.array_equal(b1, b2)
+    sides = np.array([d.nx for d in d1])
+    assert sides.min() >= 64 and sides.max() <= 1024 and np.all(sides % 32 == 0)
+    assert np.all((b1 * SQRT_4PI >= 0.5) & (b1 * SQRT_4PI <= 1.5))
+    assert set(np.unique(g1)) <= {5.0 / 3.0, 2.0}
+    cfl = np.array([d.cfl for d in d1])
+    assert cfl.min() >= 0.3 and cfl.max() <= 0.5
+
+
+def _alone(desc, b0, gamma, dtype, steps, solver=2, limiter=1):
+    ext = (desc.x_min, desc.x_max, desc.y_min, desc.y_max)
+    U = Grid2DGPU(desc.nx, desc.ny, desc.ng, *ext, dtype)
+    T = Grid2DGPU(desc.nx, desc.ny, desc.ng, *ext, dtype)
+    assert load().mhd_initialise_orszag_tang(None, C.byref(U.g), b0, gamma, None) == 0
+    ws = GpuWorkspace()
+    init_gpu_workspace(ws, U)
+    set_gpu_physics_gamma(ws, desc.gamma)
+    ws.set_limiter(limiter)
+    ws.set_cr(desc.cr)
+    info = ws.run(U, T, desc.cfl, desc.t_end, steps, solver, tuple(desc.bc))
+    out = U.download()
+    ws.destroy()
+    return out, info
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [F64, F32])
+def test_batch_equals_single_grid_runs(dtype):
+    descs = [instance(40, 40, 5 / 3, 0.4, 0.5), instance(96, 64, 2.0, 0.3, 0.5, bc=(1, 1, 2, 2)),
+             instance(33, 70, 5 / 3, 0.45, 0.5, bc=(0, 0, 1, 1)), instance(128, 128, 2.0, 0.35, 0.02)]
+    b0 = [1.0 / SQRT_4PI, 0.7 / SQRT_4PI, 1.3 / SQRT_4PI, 1.0 / SQRT_4PI]
+    gam = [d.gamma for d in descs]
+    batch = Batch(descs, dtype=dtype)
+    for i in range(len(descs)):
+        batch.init_orszag_tang(i, b0[i], gam[i])
+    infos = batch.run(25)
+    for i, d in enumerate(descs):
+        want, info = _alone(d, b0[i], gam[i], dtype, 25)
+        assert infos[i].steps == info.steps and infos[i].t == info.t, i
+        np.testing.assert_array_equal(batch.download(i), want, err_msg=f"instance {i}")
+    # the last instance has a short t_end: it stopped there, the others ran 25 steps
+    assert infos[3].t == 0.02 and infos[3].steps < 25 and infos[0].steps == 25
+    batch.destroy()
+
+
+@pytest.mark.gpu
+def test_tuning_changes_speed_not_results():
+    descs, b0, gam = orszag_tang_batch_spec(11, n=12)
+    runs = []
+    for tuning in [(8, 64), (2, 16), (16, 128)]:
+        batch = Batch(descs, dtype=F32)
+        batch.set_tuning(*tuning)
+        for i in range(len(descs)):
+            batch.init_orszag_tang(i, b0[i], gam[i])
+        batch.run(6)
+        runs.append([batch.download(i) for i in range(len(descs))])
+        batch.destroy()
+    for other in runs[1:]:
+        for a, b in zip(runs[0], other):
+            np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_autotuner_picks_a_valid_shape():
+    descs, b0, gam = orszag_tang_batch_spec(5, n=16)
+    batch = Batch(descs, dtype=F32)
+    for i in range(len(descs)):
+        batch.init_orszag_tang(i, b0[i], gam[i])
+    t = batch.tune(2)
+    assert t.xrpw in (2, 4, 8, 16) and t.yseg in (16, 32, 64, 128) and t.ctas_x > 0 and t.ctas_y > 0
+    got = batch.get_tuning()
+    assert (got.xrpw, got.yseg) == (t.xrpw, t.yseg)
+    info = batch.run(4)
+    assert all(i.steps == 4 for i in info)
+    batch.destroy()
