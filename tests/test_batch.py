@@ -54,8 +54,17 @@ def test_batch_equals_single_grid_runs(dtype):
     infos = batch.run(25)
     for i, d in enumerate(descs):
         want, info = _alone(d, b0[i], gam[i], dtype, 25)
-        assert infos[i].steps == info.steps and infos[i].t == info.t, i
-        np.testing.assert_array_equal(batch.download(i), want, err_msg=f"instance {i}")
+        got = batch.download(i)
+        assert infos[i].steps == info.steps, i
+        if dtype == F64:  # --fmad=false code: identical in every kernel that inlines it
+            assert infos[i].t == info.t, i
+            np.testing.assert_array_equal(got, want, err_msg=f"instance {i}")
+        else:  # FP32 code may contract into FMAs differently inside the batch kernels
+            assert abs(infos[i].t - info.t) <= 1e-6 * info.t, i
+            I = (slice(None), slice(2, -2), slice(2, -2))
+            num = np.abs(got[I] - want[I]).reshape(9, -1).sum(1)
+            den = np.maximum(np.abs(want[I]).reshape(9, -1).sum(1), 1e-300)
+            assert np.all(num / den <= 1e-4), (i, num / den)  # last-bit differences grown over 25 steps
     # the last instance has a short t_end: it stopped there, the others ran 25 steps
     assert infos[3].t == 0.02 and infos[3].steps < 25 and infos[0].steps == 25
     batch.destroy()
@@ -63,6 +72,7 @@ def test_batch_equals_single_grid_runs(dtype):
 
 @pytest.mark.gpu
 def test_tuning_changes_speed_not_results():
+    # the launch shape moves work between warps and CTAs but no cell's arithmetic
     descs, b0, gam = orszag_tang_batch_spec(11, n=12)
     runs = []
     for tuning in [(8, 64), (2, 16), (16, 128)]:

@@ -74,9 +74,11 @@ def test_driver_device_loop_and_fp32(tmp_path):
     devnull = open(os.devnull, "w")
     # device-resident dt (device exp for the damping factor): rounding-level agreement
     assert compare(str(tmp_path / "host"), str(tmp_path / "dev"), tol=1e-9, rtol=1e-9, out=devnull) == 0
-    # FP32-bulk against FP64, density within 1e-4 everywhere (relative L1 is checked in test_gpu_parity)
-    assert compare(str(tmp_path / "host"), str(tmp_path / "f32"), tol=1e-3, rtol=1e-2, fields=["rho"],
-                   out=devnull) == 0
+    # FP32-bulk against FP64: shock positions may shift by a cell, so compare the
+    # density in relative L1 (<= 1e-4 for this Mach-10 run to t_end)
+    a = np.loadtxt(tmp_path / "host" / "shock_bubble_mhd_gpu_t6_rho.csv", delimiter=",")
+    b = np.loadtxt(tmp_path / "f32" / "shock_bubble_mhd_gpu_t6_rho.csv", delimiter=",")
+    assert np.abs(a - b).sum() / np.abs(a).sum() <= 1e-4
 
 
 @pytest.mark.gpu
