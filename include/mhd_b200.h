@@ -247,6 +247,27 @@ int mhd_batch_set_tuning(mhd_batch* b, const mhd_batch_tuning* t);
  * fastest.  Leaves the instances one step ahead. */
 int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best);
 
+/* ---- discrete adjoint (no reference counterpart) ----
+ * Gradient of J(a) = 1/2 sum_interior (rho(t_N; a) - rho_target)^2 with respect
+ * to the 16 perturbation amplitudes a of mhd_initialise_orszag_tang
+ * (b0 = 1/sqrt(4 pi)), after nsteps steps of the split step with HLL and the
+ * given limiter on periodic [0,1]^2 (nx x ny, ng = 2).  The reverse pass
+ * differentiates the time step and c_h through the CFL argmax cell, the psi
+ * damping and every branch the forward took, recomputing the trajectory from
+ * checkpoints kept every `checkpoint_every` steps (0: about sqrt(nsteps)).
+ * dtype MHD_F64 or MHD_F32 selects the precision of forward and adjoint. */
+typedef struct mhd_adjoint mhd_adjoint;
+int mhd_adjoint_create(int nx, int ny, int dtype, int limiter, double gamma, double cfl, double cr, int nsteps,
+                       int checkpoint_every, mhd_adjoint** out);
+int mhd_adjoint_destroy(mhd_adjoint* a);
+/* rho_target: ny x nx interior densities, row-major (j * nx + i). */
+int mhd_adjoint_set_target(mhd_adjoint* a, const double* rho_target);
+/* Forward solve only: J (needs a target; else 0) and optionally the final
+ * interior density (ny x nx). */
+int mhd_adjoint_forward(mhd_adjoint* a, const double* amp16, double* J, double* rho_final);
+/* Forward solve and reverse pass: J and dJ/da (16 values). */
+int mhd_adjoint_gradient(mhd_adjoint* a, const double* amp16, double* J, double* grad16);
+
 /* ---- misc ---- */
 const char* mhd_last_error(void);
 /* Library version string. */

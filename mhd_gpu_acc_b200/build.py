@@ -36,6 +36,7 @@ CU_SOURCES = {
     "compat.cu": ["--fmad=false"],
     "ic_kernels.cu": ["--fmad=false"],
     "batch_api.cu": [],
+    "adjoint.cu": [],
 }
 CXX_SOURCES = {"cases.cpp": []}
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []

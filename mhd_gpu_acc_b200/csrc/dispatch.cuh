@@ -56,6 +56,33 @@ cudaError_t dispatch_step(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
     return with_policy<POL>(P.solver, P.limiter, go);
 }
 
+// Smallest linear interior index whose CFL speed (the forward reduction's own
+// per-cell function, floor ch) is m -- exactly for FP64; within 2^-20 relative
+// for FP32, whose code may be contracted differently in another kernel.
+// *idx must start at INT_MAX.
+template <class PH>
+__global__ void argmax_speed_kernel(DevGrid gd, double gamma, double ch, double m, int* idx) {
+    using R = typename PH::Real;
+    const double tol = sizeof(R) == 8 ? 0.0 : m * 9.5367431640625e-07;
+    const long long n = (long long)gd.nx * gd.ny;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(k / gd.nx), i = (int)(k - (long long)j * gd.nx);
+        R U[NV];
+        load_cell(gd, gd.ng + i, gd.ng + j, U);
+        if (fabs(PH::speed(U, gamma, ch) - m) <= tol) atomicMin(idx, (int)k);
+    }
+}
+
+template <class PH>
+cudaError_t launch_argmax_policy(const DevGrid& g, double gamma, double ch, double m, int* idx, cudaStream_t st) {
+    const long long n = (long long)g.nx * g.ny;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    argmax_speed_kernel<PH><<<(unsigned)blocks, 256, 0, st>>>(g, gamma, ch, m, idx);
+    return cudaGetLastError();
+}
+
 template <class PH>
 cudaError_t launch_max_policy(const DevGrid& g, double gamma, double ch, unsigned long long* out, cudaStream_t st,
                               int nsm) {

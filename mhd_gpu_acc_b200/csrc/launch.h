@@ -29,6 +29,10 @@ cudaError_t launch_max_speed_f64(const DevGrid& g, double gamma, double ch, unsi
 cudaError_t launch_max_speed_f32(const DevGrid& g, double gamma, double ch, unsigned long long* out,
                                  cudaStream_t st, int nsm);
 
+// Smallest linear interior index whose CFL speed (floor ch) equals m (atomicMin on *idx).
+cudaError_t launch_argmax_f64(const DevGrid& g, double gamma, double ch, double m, int* idx, cudaStream_t st);
+cudaError_t launch_argmax_f32(const DevGrid& g, double gamma, double ch, double m, int* idx, cudaStream_t st);
+
 // In-place apply_boundary (head/cpu/boundary_cpu.hpp:45-149), any precision.
 cudaError_t launch_apply_boundary(const DevGrid& g, int elem_bytes, const int* bc, cudaStream_t st);
 

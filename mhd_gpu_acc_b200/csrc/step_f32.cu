@@ -44,6 +44,10 @@ cudaError_t launch_batch_f32(const BatchInst* inst, const int* first, int n, int
     return dispatch_batch<FastPolicy>(inst, first, n, parity, which, solver, limiter, xrpw, yseg, ctas, st);
 }
 
+cudaError_t launch_argmax_f32(const DevGrid& g, double gamma, double ch, double m, int* idx, cudaStream_t st) {
+    return launch_argmax_policy<FastPolicy<HLL, MINMOD>>(g, gamma, ch, m, idx, st);
+}
+
 cudaError_t launch_max_speed_f32(const DevGrid& g, double gamma, double ch, unsigned long long* out,
                                  cudaStream_t st, int nsm) {
     return launch_max_policy<FastPolicy<HLL, MINMOD>>(g, gamma, ch, out, st, nsm);

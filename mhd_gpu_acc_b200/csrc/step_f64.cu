@@ -45,6 +45,10 @@ cudaError_t launch_batch_f64(const BatchInst* inst, const int* first, int n, int
     return dispatch_batch<ExactPolicy>(inst, first, n, parity, which, solver, limiter, xrpw, yseg, ctas, st);
 }
 
+cudaError_t launch_argmax_f64(const DevGrid& g, double gamma, double ch, double m, int* idx, cudaStream_t st) {
+    return launch_argmax_policy<ExactPolicy<HLL, MINMOD>>(g, gamma, ch, m, idx, st);
+}
+
 cudaError_t launch_max_speed_f64(const DevGrid& g, double gamma, double ch, unsigned long long* out,
                                  cudaStream_t st, int nsm) {
     return launch_max_policy<ExactPolicy<HLL, MINMOD>>(g, gamma, ch, out, st, nsm);
