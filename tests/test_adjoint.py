@@ -56,14 +56,14 @@ def test_gradient_matches_central_differences_small():
 
 @pytest.mark.gpu
 def test_checkpoint_interval_does_not_change_the_gradient():
-    """Recomputation from checkpoints reproduces the trajectory bit for bit; the
-    gradient agrees to the rounding of its atomically summed dt / c_h cotangents."""
+    """Recomputation from checkpoints reproduces the trajectory bit for bit; J and
+    the gradient agree to the rounding of their atomically summed reductions."""
     ref, a = _problem(48, 30, every=1)
     J1, g1 = ref.gradient(a)
     for every in (5, 7, 30):
         adj, _ = _problem(48, 30, every=every)
         J2, g2 = adj.gradient(a)
-        assert J1 == J2
+        assert abs(J1 - J2) <= 1e-14 * abs(J1)
         np.testing.assert_allclose(g2, g1, rtol=1e-10, atol=1e-14 * np.abs(g1).max())
 
 
