@@ -108,6 +108,10 @@ int mhd_get_ch(const mhd_workspace* ws, double* ch);
 int mhd_set_limiter(mhd_workspace* ws, int limiter);
 /* GLM damping ratio c_r = c_p^2 / c_h (default 0.18, head/physics.hpp:39). */
 int mhd_set_cr(mhd_workspace* ws, double cr);
+/* Launch shape of the sweeps (no reference counterpart; results do not depend
+ * on it): x-sweep rows per warp (default 8) and the height of the row band one
+ * y-sweep warp marches down (default 32). */
+int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband);
 
 /* Replaces compute_dt_gpu (src/gpu/solver_gpu.cu:578-605): CFL maximum over the
  * interior floored by the current ch; sets ch to it and returns

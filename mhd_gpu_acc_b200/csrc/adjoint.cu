@@ -426,8 +426,8 @@ int reverse_step(mhd_adjoint* a, int n, const mhd_grid& Un, const mhd_grid& Un1,
         mhd::StepParams P{};
         P.gamma = a->gamma; P.cr = a->cr; P.dx = dx; P.dy = dy; P.dmin = dx < dy ? dx : dy;
         P.dt = dt; P.ch = ch; P.damp = f; P.solver = MHD_HLL; P.limiter = a->limiter;
-        const cudaError_t e = f64(a) ? mhd::launch_step_f64(dg(Un), dg(a->T), dg(a->T), P, st, 64, 1)
-                                     : mhd::launch_step_f32(dg(Un), dg(a->T), dg(a->T), P, st, 64, 1);
+        const cudaError_t e = f64(a) ? mhd::launch_step_f64(dg(Un), dg(a->T), dg(a->T), P, st, mhd::kDefaultYBand, 1)
+                                     : mhd::launch_step_f32(dg(Un), dg(a->T), dg(a->T), P, st, mhd::kDefaultYBand, 1);
         ACK(e);
     }
     // (c) lambda_T = Y^T lambda_V

@@ -72,8 +72,13 @@ __global__ void __launch_bounds__(32 * YS_WARPS) batch_y_kernel(const BatchInst*
             continue;
         }
         const int strips = inst[k].y_strips;
-        y_segment<PH>(inst[k].T, inst[k].U, P, dt, ch, damp, local % strips,
-                      (local / strips) * YS_WARPS + threadIdx.y, seg);
+        const DevGrid& T = inst[k].T;
+        const int r0 = ((local / strips) * YS_WARPS + threadIdx.y) * seg;
+        double vmax = 0.0;
+        unsigned reverts = 0;
+        y_segment<PH>(T, inst[k].U, P, dt, ch, damp, local % strips, T.ng + r0, min(seg, T.ny - r0), vmax,
+                      reverts);
+        y_fold(P, vmax, reverts);
         if (local == 0 && lead) clock_advance(P, dt, ch);
     }
 }

@@ -82,7 +82,7 @@ int build_worklist(mhd_batch* b) {
         I.x_tiles = (b->desc[i].nx + mhd::XS_TX - 1) / mhd::XS_TX;
         const int rows = mhd::XS_ROWS * b->tune.xrpw;
         I.x_rblocks = (b->desc[i].ny + rows - 1) / rows;
-        I.y_strips = (b->desc[i].nx + 2 * b->desc[i].ng + 31) / 32;
+        I.y_strips = (b->desc[i].nx + b->desc[i].ng + 31) / 32;  // strips holding interior columns
         const int nseg = (b->desc[i].ny + b->tune.yseg - 1) / b->tune.yseg;
         I.y_groups = (nseg + mhd::YS_WARPS - 1) / mhd::YS_WARPS;
         b->first[i + 1] = b->first[i] + I.x_tiles * I.x_rblocks;

@@ -97,7 +97,8 @@ struct mhd_workspace {
     double ch = 0.0;
     double cr = 0.18;          // head/physics.hpp:39
     int limiter = MHD_LIMITER_MINMOD;
-    int yseg = 64;
+    int yseg = mhd::kDefaultYBand;  // y-sweep rows per warp band
+    int xrpw = mhd::kDefaultXRpw;  // x-sweep rows per warp
     int nsm = 148;
     cudaStream_t stream = nullptr;
     unsigned long long* d_max = nullptr;
@@ -108,7 +109,7 @@ struct mhd_workspace {
     // graph of two captured steps
     cudaGraphExec_t graph = nullptr;
     struct Key {
-        void* u; void* t; int solver, limiter, bc[4], yseg;
+        void* u; void* t; int solver, limiter, bc[4], yseg, xrpw;
         double gamma, cr, cfl, t_end;
         bool operator==(const Key& o) const { return std::memcmp(this, &o, sizeof(Key)) == 0; }
     } key{};
@@ -152,10 +153,11 @@ mhd::StepParams base_params(const mhd_workspace* ws, const mhd_grid* g, int solv
 }
 
 cudaError_t launch_step(const mhd_grid* g, const mhd::DevGrid& in, const mhd::DevGrid& tmp, const mhd::DevGrid& out,
-                        const mhd::StepParams& P, cudaStream_t st, int yseg, int which = 3) {
+                        const mhd::StepParams& P, cudaStream_t st, int yseg, int which = 3,
+                        int xrpw = mhd::kDefaultXRpw) {
     g_launches += (which == 3) ? 2 : 1;
-    return g->dtype == MHD_F64 ? mhd::launch_step_f64(in, tmp, out, P, st, yseg, which)
-                               : mhd::launch_step_f32(in, tmp, out, P, st, yseg, which);
+    return g->dtype == MHD_F64 ? mhd::launch_step_f64(in, tmp, out, P, st, yseg, which, xrpw)
+                               : mhd::launch_step_f32(in, tmp, out, P, st, yseg, which, xrpw);
 }
 
 cudaError_t launch_max(const mhd_workspace* ws, const mhd_grid* g, cudaStream_t st) {
@@ -407,6 +409,15 @@ int mhd_set_cr(mhd_workspace* ws, double cr) {
     return MHD_OK;
 }
 
+int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband) {
+    if (!ws) return fail(MHD_ERR_STATE, "mhd_set_sweep_shape: null workspace");
+    if (xrpw < 1 || xrpw > 64 || yband < 1 || yband > 65536)
+        return fail(MHD_ERR_ARG, "mhd_set_sweep_shape: need 1 <= xrpw <= 64 and 1 <= yband <= 65536");
+    ws->xrpw = xrpw;
+    ws->yseg = yband;
+    return MHD_OK;
+}
+
 int mhd_compute_dt(mhd_workspace* ws, const mhd_grid* g, double cfl, double* dt) {
     int rc = check_ws_grid(ws, g, "mhd_compute_dt");
     if (rc) return rc;
@@ -447,7 +458,7 @@ int mhd_advance(mhd_workspace* ws, const mhd_grid* Uold, mhd_grid* Utmp, mhd_gri
     if (P.damp >= 1.0) P.damp = 1.0;
     P.t_end = 0.0;
     P.cfl = 0.0;
-    CK(launch_step(Uold, dev(Uold), dev(Utmp), dev(Unew), P, ws->stream, ws->yseg));
+    CK(launch_step(Uold, dev(Uold), dev(Utmp), dev(Unew), P, ws->stream, ws->yseg, 3, ws->xrpw));
     return MHD_OK;
 }
 
@@ -502,7 +513,7 @@ int mhd_profile_sweeps(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, 
         mhd::StepParams Q = P;
         Q.parity = r & 1;
         cudaEventRecord(ev[0], st);
-        e = launch_step(U, dU, dT, dU, Q, st, ws->yseg, 1);
+        e = launch_step(U, dU, dT, dU, Q, st, ws->yseg, 1, ws->xrpw);
         cudaEventRecord(ev[1], st);
         if (e == cudaSuccess) e = launch_step(U, dU, dT, dU, Q, st, ws->yseg, 2);
         cudaEventRecord(ev[2], st);
@@ -530,7 +541,7 @@ int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_en
     mhd_workspace::Key key{};
     key.u = U->data; key.t = T->data; key.solver = solver; key.limiter = ws->limiter;
     for (int k = 0; k < 4; ++k) key.bc[k] = bc[k];
-    key.yseg = ws->yseg; key.gamma = ws->gamma; key.cr = ws->cr; key.cfl = cfl; key.t_end = t_end;
+    key.yseg = ws->yseg; key.xrpw = ws->xrpw; key.gamma = ws->gamma; key.cr = ws->cr; key.cfl = cfl; key.t_end = t_end;
     const mhd::DevGrid dU = dev(U), dT = dev(T);
     if (!ws->graph || !(ws->key == key)) {
         if (ws->graph) { cudaGraphExecDestroy(ws->graph); ws->graph = nullptr; }
@@ -546,8 +557,8 @@ int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_en
         for (int par = 0; par < 2 && e1 == cudaSuccess; ++par) {
             mhd::StepParams Q = P;
             Q.parity = par;
-            e1 = (U->dtype == MHD_F64) ? mhd::launch_step_f64(dU, dT, dU, Q, cap, ws->yseg, 3)
-                                       : mhd::launch_step_f32(dU, dT, dU, Q, cap, ws->yseg, 3);
+            e1 = (U->dtype == MHD_F64) ? mhd::launch_step_f64(dU, dT, dU, Q, cap, ws->yseg, 3, ws->xrpw)
+                                       : mhd::launch_step_f32(dU, dT, dU, Q, cap, ws->yseg, 3, ws->xrpw);
         }
         e2 = cudaStreamEndCapture(cap, &gr);
         if (own) cudaStreamDestroy(cap);
@@ -571,7 +582,7 @@ int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_en
         if (max_steps & 1) {
             mhd::StepParams Q = P;
             Q.parity = 0;
-            CK(launch_step(U, dU, dT, dU, Q, st, ws->yseg));
+            CK(launch_step(U, dU, dT, dU, Q, st, ws->yseg, 3, ws->xrpw));
         }
         CK(cudaMemcpyAsync(&hc, ws->d_clock, sizeof hc, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

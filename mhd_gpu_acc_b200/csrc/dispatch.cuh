@@ -1,7 +1,8 @@
 // dispatch.cuh -- runtime (solver, limiter) -> template instance dispatch and
 // launch geometry of the two sweeps, shared by the FP64 and FP32 translation
 // units.  `which` selects the sweeps: 1 = x only, 2 = y only, 3 = both;
-// `yseg` is the y-sweep segment length and `xrpw` the x-sweep rows per warp.
+// `yband` is the height of a y-sweep warp's row band and `xrpw` the x-sweep rows
+// per warp.
 #pragma once
 
 #include "sweep.cuh"
@@ -10,16 +11,17 @@ namespace mhd {
 
 template <class PH>
 cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                          cudaStream_t st, int yseg, int which, int xrpw) {
+                          cudaStream_t st, int yband, int which, int xrpw) {
     if (which & 1) {
         const int rows_per_cta = XS_ROWS * xrpw;
         const dim3 bx(32 * XS_ROWS), gx((in.nx + XS_TX - 1) / XS_TX, (in.ny + rows_per_cta - 1) / rows_per_cta);
         sweep_x_kernel<PH><<<gx, bx, 0, st>>>(in, tmp, P, xrpw);
     }
     if (which & 2) {
-        const int nseg = (in.ny + yseg - 1) / yseg;
-        const dim3 by(32, YS_WARPS), gy((in.tnx() + 31) / 32, (nseg + YS_WARPS - 1) / YS_WARPS);
-        sweep_y_kernel<PH><<<gy, by, 0, st>>>(tmp, out, P, yseg);
+        const int per = yband > 0 ? yband : kDefaultYBand;
+        const long long warps = (long long)y_strips(tmp) * ((tmp.ny + per - 1) / per);
+        const unsigned grid = (unsigned)((warps + YS_WARPS - 1) / YS_WARPS);
+        sweep_y_kernel<PH><<<grid, dim3(32, YS_WARPS), 0, st>>>(tmp, out, P, per);
     }
     return cudaGetLastError();
 }

@@ -120,8 +120,8 @@ extern "C" int mhd_advance_noalloc(const mhd_grid* Uold, mhd_grid* Unew, double 
     P.any_dirichlet = (bc[0] == MHD_BC_DIRICHLET || bc[1] == MHD_BC_DIRICHLET || bc[2] == MHD_BC_DIRICHLET ||
                        bc[3] == MHD_BC_DIRICHLET);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const cudaError_t e = (Uold->dtype == MHD_F64) ? mhd::launch_step_f64(in, tmp, out, P, st, 64, 3)
-                                                   : mhd::launch_step_f32(in, tmp, out, P, st, 64, 3);
+    const cudaError_t e = (Uold->dtype == MHD_F64) ? mhd::launch_step_f64(in, tmp, out, P, st, mhd::kDefaultYBand, 3)
+                                                   : mhd::launch_step_f32(in, tmp, out, P, st, mhd::kDefaultYBand, 3);
     if (e != cudaSuccess) return err(MHD_ERR_CUDA, "mhd_advance_noalloc: launch failed (%lld)", (long long)e);
     return MHD_OK;
 }

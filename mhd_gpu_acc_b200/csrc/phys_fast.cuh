@@ -27,11 +27,6 @@ constexpr float kLowBetaFrac = 0.02f;
 // x * 0 is 0 for finite x and NaN for an infinity or a NaN, so an FMA chain of
 // the values times zero tells whether all are finite with FMA-pipe work and a
 // single comparison (instead of one ALU test per value).
-__device__ __forceinline__ bool all_finite(const float* v, int n) {
-    float z = v[0] * 0.0f;
-    for (int k = 1; k < n; ++k) z = fmaf(v[k], 0.0f, z);
-    return z == 0.0f;
-}
 __device__ __forceinline__ bool both_finite(float a, float b) { return fmaf(a, 0.0f, b * 0.0f) == 0.0f; }
 
 struct Side {
@@ -380,63 +375,141 @@ __device__ __forceinline__ float vanleer(float a, float b) {
     return 2.0f * ab / (a + b);
 }
 
-__device__ __forceinline__ bool is_physical(const float* V) {
-    return V[RHO] > kRhoFloor && V[PP] > kPFloor && all_finite(V, NV);
+// ---------------------------------------------------------------------------
+// Packed face pairs.  A cell's MUSCL-Hancock predictor produces its left-face
+// and right-face states together and treats them identically, so they are
+// carried as float2 (.x = left face, .y = right face) and advanced with the
+// sm_100 paired FP32 instructions (one issue slot for both faces).  Per
+// component the arithmetic is the scalar code's (round-to-nearest FMA / add /
+// multiply), only the contraction pattern differs.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(1.0f / a.x, 1.0f / a.y); }
+
+// p2c of both faces.
+__device__ __forceinline__ void p2c2(const float2* W, float inv_gm1, float2* U) {
+    const float2 B2 = fma2(W[BZ], W[BZ], fma2(W[BY], W[BY], mul2(W[BX], W[BX])));
+    const float2 v2 = fma2(W[PW], W[PW], fma2(W[PV], W[PV], mul2(W[PU], W[PU])));
+    const float2 half = dup2(0.5f);
+    U[RHO] = W[RHO];
+    U[MX] = mul2(W[RHO], W[PU]); U[MY] = mul2(W[RHO], W[PV]); U[MZ] = mul2(W[RHO], W[PW]);
+    U[BX] = W[BX]; U[BY] = W[BY]; U[BZ] = W[BZ];
+    U[EN] = fma2(W[PP], dup2(inv_gm1), fma2(half, B2, mul2(mul2(half, W[RHO]), v2)));
+    U[PSI] = W[PSI];
 }
 
-// MUSCL-Hancock half step (src/cpu/solver_cpu.cpp:88-119; c_h in the predictor).
+// GLM-MHD physical flux of both faces from consistent (U, W) pairs.
+template <int DIR>
+__device__ __forceinline__ void flux2(const float2* U, const float2* W, float ch, float2* F) {
+    const float2 B2 = fma2(W[BZ], W[BZ], fma2(W[BY], W[BY], mul2(W[BX], W[BX])));
+    const float2 pt = fma2(dup2(0.5f), B2, W[PP]);
+    const float2 uB = fma2(W[PW], W[BZ], fma2(W[PV], W[BY], mul2(W[PU], W[BX])));
+    const float2 c2 = dup2(ch * ch);
+    if (DIR == 0) {
+        F[0] = U[MX];
+        F[1] = fma2(U[MX], W[PU], sub2(pt, mul2(W[BX], W[BX])));
+        F[2] = fma2(U[MX], W[PV], mul2(make_float2(-W[BX].x, -W[BX].y), W[BY]));
+        F[3] = fma2(U[MX], W[PW], mul2(make_float2(-W[BX].x, -W[BX].y), W[BZ]));
+        F[4] = W[PSI];
+        F[5] = fma2(W[BY], W[PU], mul2(make_float2(-W[BX].x, -W[BX].y), W[PV]));
+        F[6] = fma2(W[BZ], W[PU], mul2(make_float2(-W[BX].x, -W[BX].y), W[PW]));
+        F[7] = fma2(add2(U[EN], pt), W[PU], mul2(make_float2(-W[BX].x, -W[BX].y), uB));
+        F[8] = mul2(c2, W[BX]);
+    } else {
+        F[0] = U[MY];
+        F[1] = fma2(U[MY], W[PU], mul2(make_float2(-W[BY].x, -W[BY].y), W[BX]));
+        F[2] = fma2(U[MY], W[PV], sub2(pt, mul2(W[BY], W[BY])));
+        F[3] = fma2(U[MY], W[PW], mul2(make_float2(-W[BY].x, -W[BY].y), W[BZ]));
+        F[4] = fma2(W[BX], W[PV], mul2(make_float2(-W[BY].x, -W[BY].y), W[PU]));
+        F[5] = W[PSI];
+        F[6] = fma2(W[BZ], W[PV], mul2(make_float2(-W[BY].x, -W[BY].y), W[PW]));
+        F[7] = fma2(add2(U[EN], pt), W[PV], mul2(make_float2(-W[BY].x, -W[BY].y), uB));
+        F[8] = mul2(c2, W[BY]);
+    }
+}
+
+// Scalar FP64 pressure recovery of one face (the flagged low-internal-energy branch of c2p).
+__device__ __forceinline__ float eint_fp64(float r, float mx, float my, float mz, float bx, float by, float bz, float E) {
+    const double ke = 0.5 * ((double)mx * mx + (double)my * my + (double)mz * mz) / (double)r;
+    return (float)((double)E - ke - 0.5 * ((double)bx * bx + (double)by * by + (double)bz * bz));
+}
+
+// c2p of both faces, with c2p's FP64 branch per face.
+__device__ __forceinline__ void c2p2(const float2* U, float gm1, float2* W) {
+    const float2 inv_rho = rcp2(U[RHO]);
+    const float2 ux = mul2(U[MX], inv_rho), uy = mul2(U[MY], inv_rho), uz = mul2(U[MZ], inv_rho);
+    const float2 B2 = fma2(U[BZ], U[BZ], fma2(U[BY], U[BY], mul2(U[BX], U[BX])));
+    const float2 mu = fma2(U[MZ], uz, fma2(U[MY], uy, mul2(U[MX], ux)));
+    float2 eint = fma2(dup2(-0.5f), add2(mu, B2), U[EN]);
+    const float2 lim = mul2(dup2(kLowBetaFrac), U[EN]);
+    if (eint.x < lim.x)
+        eint.x = eint_fp64(U[RHO].x, U[MX].x, U[MY].x, U[MZ].x, U[BX].x, U[BY].x, U[BZ].x, U[EN].x);
+    if (eint.y < lim.y)
+        eint.y = eint_fp64(U[RHO].y, U[MX].y, U[MY].y, U[MZ].y, U[BX].y, U[BY].y, U[BZ].y, U[EN].y);
+    W[RHO] = U[RHO]; W[PU] = ux; W[PV] = uy; W[PW] = uz;
+    W[BX] = U[BX]; W[BY] = U[BY]; W[BZ] = U[BZ]; W[PP] = mul2(dup2(gm1), eint); W[PSI] = U[PSI];
+}
+
+// is_physical (rho and p above their floors, every value finite) of both faces.
+__device__ __forceinline__ void is_physical2(const float2* V, bool& okx, bool& oky) {
+    float2 z = mul2(V[0], dup2(0.0f));
+#pragma unroll
+    for (int k = 1; k < NV; ++k) z = fma2(V[k], dup2(0.0f), z);
+    okx = V[RHO].x > kRhoFloor && V[PP].x > kPFloor && z.x == 0.0f;
+    oky = V[RHO].y > kRhoFloor && V[PP].y > kPFloor && z.y == 0.0f;
+}
+
+// MUSCL-Hancock half step (src/cpu/solver_cpu.cpp:88-119; c_h in the predictor)
+// on packed face pairs.  The fallbacks (first-order face values, or the
+// unadvanced face state) are rare, so they are taken as a branch guarded by a
+// vote of the active lanes instead of as per-component selects.
 template <int DIR, int LIMITER>
 __device__ __forceinline__ void reconstruct(const float* Wm, const float* Wc, const float* Wp, float dtd, float ch,
                                             float g, Side& Ls, Side& Rs) {
-    float* WL = Ls.W();
-    float* WR = Rs.W();
+    float2 W[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
         const float a = Wc[k] - Wm[k], b = Wp[k] - Wc[k];
         const float s = (LIMITER == VANLEER) ? vanleer(a, b) : minmod(a, b);
-        WL[k] = Wc[k] - 0.5f * s;
-        WR[k] = Wc[k] + 0.5f * s;
+        W[k] = fma2(make_float2(-0.5f, 0.5f), dup2(s), dup2(Wc[k]));
     }
-    if (!is_physical(WL)) {
+    const unsigned active = __activemask();
+    bool okL, okR;
+    is_physical2(W, okL, okR);
+    if (__any_sync(active, !(okL && okR))) {
 #pragma unroll
-        for (int k = 0; k < NV; ++k) WL[k] = Wc[k];
+        for (int k = 0; k < NV; ++k) {
+            if (!okL) W[k].x = Wc[k];
+            if (!okR) W[k].y = Wc[k];
+        }
     }
-    if (!is_physical(WR)) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) WR[k] = Wc[k];
-    }
-    float UL[NV], UR[NV], FL[NV], FR[NV];
-    p2c(WL, g, UL);
-    p2c(WR, g, UR);
-    flux<DIR>(UL, WL, ch, FL);
-    flux<DIR>(UR, WR, ch, FR);
+    float2 U0[NV], F[NV];
+    p2c2(W, 1.0f / (g - 1.0f), U0);
+    flux2<DIR>(U0, W, ch, F);
     const float s = 0.5f * dtd;
-    float V[NV];
-    {
-        float* U = Ls.U();
+    float2 U[NV], V[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) U[k] = UL[k] - s * (FR[k] - FL[k]);
-        c2p(U, g, V);
-        if (is_physical(V)) {
+    for (int k = 0; k < NV; ++k) {
+        const float d = s * (F[k].y - F[k].x);
+        U[k] = make_float2(U0[k].x - d, U0[k].y - d);
+    }
+    c2p2(U, g - 1.0f, V);
+    is_physical2(V, okL, okR);
+    if (__any_sync(active, !(okL && okR))) {
 #pragma unroll
-            for (int k = 0; k < NV; ++k) WL[k] = V[k];
-        } else {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) U[k] = UL[k];  // WL already matches UL
+        for (int k = 0; k < NV; ++k) {
+            if (!okL) { V[k].x = W[k].x; U[k].x = U0[k].x; }
+            if (!okR) { V[k].y = W[k].y; U[k].y = U0[k].y; }
         }
     }
-    {
-        float* U = Rs.U();
 #pragma unroll
-        for (int k = 0; k < NV; ++k) U[k] = UR[k] - s * (FR[k] - FL[k]);
-        c2p(U, g, V);
-        if (is_physical(V)) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) WR[k] = V[k];
-        } else {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) U[k] = UR[k];
-        }
+    for (int k = 0; k < NV; ++k) {
+        Ls.U()[k] = U[k].x; Ls.W()[k] = V[k].x;
+        Rs.U()[k] = U[k].y; Rs.W()[k] = V[k].y;
     }
 }
 

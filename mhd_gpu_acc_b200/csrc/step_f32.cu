@@ -15,6 +15,7 @@ struct FastPolicy {
     using Real = float;
     static constexpr int NW = NV;
     static constexpr int NS = 2 * NV;
+    static constexpr int kYBlocks = 3;  // y-sweep CTAs per SM the register budget is cut for
     struct Prim { float v[NV]; };
     using Side = fast::Side;
 

@@ -16,6 +16,7 @@ struct ExactPolicy {
     using Real = double;
     static constexpr int NW = NV;  // primitive values per cell
     static constexpr int NS = NV;  // values per reconstructed side state (U*)
+    static constexpr int kYBlocks = 2;  // y-sweep CTAs per SM the register budget is cut for
     struct Prim { double v[NV]; };
     struct Side { double v[NV]; };
 

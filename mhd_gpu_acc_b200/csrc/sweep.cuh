@@ -32,9 +32,9 @@ namespace mhd {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int XS_TX = 28;       // interior cells per warp in the x-sweep (32 lanes - 4 halo)
 constexpr int XS_ROWS = 8;      // warps (rows) per x-sweep CTA
-// rows each x-sweep warp processes (with one-row prefetch) and rows per y-sweep
-// warp segment are launch parameters; their defaults are kDefaultXRpw and
-// kDefaultYSeg (mhd_common.cuh), the autotuner may pick others.
+// rows each x-sweep warp processes (with one-row prefetch) and the rows a
+// y-sweep warp takes are launch parameters (kDefaultXRpw, kDefaultYBand and, for
+// batches, kDefaultYSeg in mhd_common.cuh; the batch autotuner may pick others).
 constexpr int YS_WARPS = 4;     // warps (row segments) per y-sweep CTA
 
 template <int N, typename T>
@@ -64,8 +64,10 @@ __device__ __forceinline__ void store_cell(const DevGrid& g, int x, int y, const
 
 // Writes interior cell (x, y)'s value to every ghost cell of `out` whose
 // boundary rule copies it (non-Dirichlet sides), corners by composition.
+// Inlined (on the rare near-edge path) so that neither the cell nor the kernel
+// parameter block holding `bc` has to be spilled to the stack for a call.
 template <typename R>
-__device__ __noinline__ void scatter_ghosts(const DevGrid& out, int x, int y, const R* v, const int* bc) {
+__device__ __forceinline__ void scatter_ghosts(const DevGrid& out, int x, int y, const R* v, const int* bc) {
     const int ng = out.ng, ib = ng, ie = ng + out.nx, jb = ng, je = ng + out.ny;
     for (int a = 0; a <= 2 * ng; ++a) {
         int gx = x, fx = 0;
@@ -111,7 +113,7 @@ __device__ __forceinline__ bool near_edge(const DevGrid& g, int x, int y) {
 // sides (copy_ghost_cells) and corners whose rule passes through a Dirichlet
 // side.  Grid-stride over all ghost cells.
 template <typename R>
-__device__ void gather_dirichlet_ghosts(const DevGrid& in, const DevGrid& out, const int* bc) {
+__device__ __forceinline__ void gather_dirichlet_ghosts(const DevGrid& in, const DevGrid& out, const int* bc) {
     const int ng = in.ng, ib = ng, ie = ng + in.nx, jb = ng, je = ng + in.ny;
     const int tx = in.tnx(), ty = in.tny();
     const long long nthreads = (long long)gridDim.x * gridDim.y * blockDim.x * blockDim.y;
@@ -122,20 +124,20 @@ __device__ void gather_dirichlet_ghosts(const DevGrid& in, const DevGrid& out, c
         const int y = (int)(k / tx), x = (int)(k - (long long)y * tx);
         const bool xg = (x < ib || x >= ie), yg = (y < jb || y >= je);
         if (!xg && !yg) continue;
-        const int sx_side = (x < ib) ? 0 : 1, sy_side = (y < jb) ? 2 : 3;
+        const int bcx = (x < ib) ? bc[0] : bc[1], bcy = (y < jb) ? bc[2] : bc[3];
         int srcx = x, srcy = y, fx = 0, fy = 0;
         if (xg && !yg) {
-            if (bc[sx_side] != DIRICHLET) continue;
+            if (bcx != DIRICHLET) continue;
         } else if (yg && !xg) {
-            if (bc[sy_side] != DIRICHLET) continue;
+            if (bcy != DIRICHLET) continue;
         } else {
-            if (bc[sy_side] != DIRICHLET) {
-                if (bc[sx_side] != DIRICHLET) continue;  // produced by the scatter
+            if (bcy != DIRICHLET) {
+                if (bcx != DIRICHLET) continue;  // produced by the scatter
                 srcy = ghost_src_y(y, jb, je, bc);
-                fy = (bc[sy_side] == REFLECTING);
-            } else if (bc[sx_side] != DIRICHLET) {
+                fy = (bcy == REFLECTING);
+            } else if (bcx != DIRICHLET) {
                 srcx = ghost_src_x(x, ib, ie, bc);
-                fx = (bc[sx_side] == REFLECTING);
+                fx = (bcx == REFLECTING);
             }
         }
         R w[NV];
@@ -246,23 +248,22 @@ __global__ void __launch_bounds__(32 * XS_ROWS) sweep_x_kernel(DevGrid in, DevGr
 // ---------------------------------------------------------------------------
 // y-sweep
 // ---------------------------------------------------------------------------
-// One warp marches down rows [j0, j0 + seg) of a 32-column strip (lane = column
-// x = strip*32 + lane), then folds its CFL maximum into one atomic (when
-// P.accumulate) and its revert count into the clock.  Called by whole warps.
+// One warp marches down interior rows [j0, j0 + count) (ghost offset included)
+// of a 32-column strip (lane = column x = strip*32 + lane), folding the CFL
+// speed of every updated cell into vmax (when P.accumulate) and counting
+// reverted cells.  Called by whole warps; y_fold publishes the two results.
 template <class PH>
 __device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out, const StepParams& P, double dt,
-                                          double ch, double damp, int strip, int seg_index, int seg) {
+                                          double ch, double damp, int strip, int j0, int count, double& vmax,
+                                          unsigned& reverts) {
     using R = typename PH::Real;
     const int lane = threadIdx.x & 31;
-    const int ng = in.ng, ib = ng, ie = ng + in.nx, jb = ng, je = ng + in.ny;
+    const int ng = in.ng, ib = ng, ie = ng + in.nx;
     const int x = strip * 32 + lane;
-    const int j0 = jb + seg_index * seg;
-    const int j1 = min(j0 + seg, je);
-    const bool active = (x >= ib && x < ie && j0 < je);
+    const int j1 = j0 + count;
+    const bool active = (x >= ib && x < ie && count > 0);
     const double g = P.gamma;
     const double dtd = dt / P.dy;
-    double vmax = 0.0;
-    unsigned reverts = 0;
 
     if (active) {
         typename PH::Prim Wm, Wc, Wp;
@@ -305,6 +306,12 @@ __device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out,
             Wc = Wp;
         }
     }
+}
+
+// Warp-wide CFL maximum into one atomic (when P.accumulate) and the revert
+// count into the clock.  Called by whole warps.
+__device__ __forceinline__ void y_fold(const StepParams& P, double vmax, unsigned reverts) {
+    const int lane = threadIdx.x & 31;
     if (P.accumulate) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -328,17 +335,34 @@ __device__ __forceinline__ void clock_advance(const StepParams& P, double dt, do
     c->last_ch = ch;
 }
 
+// The y-sweep's work is `strips` column strips, each cut into row bands of
+// `per` rows (32 by default).  Warp w takes strip w % strips, band w / strips:
+// the warps of a CTA sit side by side on one band and consecutive CTAs walk
+// across the width first, so the resident CTAs cover a narrow window of
+// full-width rows that moves down the grid.  Measured on B200 (4096^2, FP32):
+// 32-row bands 0.72 ms, 64 rows 0.78 ms, 128 rows 0.96 ms, and one wave of
+// ~300-row bands 1.31 ms -- short bands in a moving window keep the segment
+// halos and the pages in use shared.
+__host__ __device__ __forceinline__ int y_strips(const DevGrid& g) { return (g.ng + g.nx + 31) / 32; }
+
 template <class PH>
-__global__ void __launch_bounds__(32 * YS_WARPS) sweep_y_kernel(DevGrid in, DevGrid out, StepParams P, int seg) {
+__global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) sweep_y_kernel(DevGrid in, DevGrid out,
+                                                                            StepParams P, int per) {
     using R = typename PH::Real;
     double dt, ch, damp;
-    const bool first = (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0);
+    const bool first = (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0);
     if (!step_scalars(P, dt, ch, damp)) {
         if (first) clock_flag_skip(P);
         return;
     }
     if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
-    y_segment<PH>(in, out, P, dt, ch, damp, blockIdx.x, blockIdx.y * YS_WARPS + threadIdx.y, seg);
+    const int strips = y_strips(in);
+    const int w = blockIdx.x * YS_WARPS + threadIdx.y;
+    const int r0 = (w / strips) * per;
+    double vmax = 0.0;
+    unsigned reverts = 0;
+    if (r0 < in.ny) y_segment<PH>(in, out, P, dt, ch, damp, w % strips, in.ng + r0, min(per, in.ny - r0), vmax, reverts);
+    y_fold(P, vmax, reverts);
     if (P.clock && first) clock_advance(P, dt, ch);
 }
 

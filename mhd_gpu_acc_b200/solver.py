@@ -219,6 +219,10 @@ class GpuWorkspace:
     def set_cr(self, cr: float) -> None:
         check(load().mhd_set_cr(self._req(), float(cr)), "mhd_set_cr")
 
+    def set_sweep_shape(self, xrpw: int = 8, yband: int = 32) -> None:
+        """Launch shape only: x-sweep rows per warp, y-sweep rows per warp band."""
+        check(load().mhd_set_sweep_shape(self._req(), int(xrpw), int(yband)), "mhd_set_sweep_shape")
+
     @property
     def ch(self) -> float:
         v = C.c_double()
