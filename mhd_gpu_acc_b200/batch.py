@@ -37,6 +37,26 @@ def orszag_tang_batch_spec(seed: int, n: int = 256, t_end: float = 0.5):
     return descs, b0, gam
 
 
+def lpt_partition(weights, parts: int) -> list[list[int]]:
+    """Longest-processing-time-first split of independent instances over `parts`
+    GPUs: instances in decreasing weight (cells; ties by index) go one by one to
+    the part with the least weight so far (lowest part on ties).  Deterministic,
+    so every rank computes the same plan without communication; each part's
+    index list is returned sorted.  The heaviest part exceeds the lightest by at
+    most the largest single weight."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    w = [float(x) for x in weights]
+    order = sorted(range(len(w)), key=lambda i: (-w[i], i))
+    load = [0.0] * parts
+    out: list[list[int]] = [[] for _ in range(parts)]
+    for i in order:
+        p = min(range(parts), key=lambda q: (load[q], q))
+        out[p].append(i)
+        load[p] += w[i]
+    return [sorted(s) for s in out]
+
+
 class Batch:
     def __init__(self, descs, dtype=F32, solver=2, limiter=1):
         self.n = len(descs)
