@@ -57,6 +57,10 @@ def parse():
                          "adjoint: gradient of the Orszag-Tang objective")
     ap.add_argument("--seed", type=int, default=0, help="batch workload seed")
     ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--xrpw", type=int, default=8, help="x-sweep rows per warp")
+    ap.add_argument("--yband", type=int, default=32, help="y-sweep rows per warp band")
+    ap.add_argument("--ystage", type=int, default=0, choices=[0, 1],
+                    help="y-sweep rows: 0 per-thread loads, 1 TMA-staged shared-memory boxes")
     return ap.parse_args()
 
 
@@ -258,6 +262,7 @@ def run_ours(a, world, rank, local):
         m.set_gpu_physics_gamma(ws, cfg.gamma)
         m.set_gpu_physics_ch(ws, 0.0)
         ws.set_limiter(limiter)
+        ws.set_sweep_shape(a.xrpw, a.yband, a.ystage)
         ws.set_stream(stream.cuda_stream)
         U.upload(U0)
         ws.run(U, T, cfg.cfl, t_end, a.warmup, solver, bc)
@@ -332,6 +337,7 @@ def run_ours(a, world, rank, local):
         m.init_gpu_workspace(ws, U)
         m.set_gpu_physics_gamma(ws, cfg.gamma)
         ws.set_limiter(limiter)
+        ws.set_sweep_shape(a.xrpw, a.yband, a.ystage)
         ws.set_stream(stream.cuda_stream)
         hin = torch.from_numpy(U0).pin_memory()
         hout = torch.empty_like(hin).pin_memory()
@@ -375,7 +381,9 @@ def run_ours(a, world, rank, local):
             "config": {"workload": f"orszag_tang_unit_{n}x{n}_hlld_vanleer_cfl0.4", "nx": n, "ny": n,
                        "solver": "hlld", "limiter": "vanleer", "precision": "fp32-bulk (fp64 low-beta pressure, "
                        "fp64 dt reduction)", "per_gpu": "one independent instance",
-                       "l2": "state 604 MB (fp32) / 1.2 GB (fp64) > 126 MB L2; no flush"},
+                       "l2": "state 604 MB (fp32) / 1.2 GB (fp64) > 126 MB L2; no flush",
+                       "sweep_shape": {"xrpw": a.xrpw, "yband": a.yband,
+                                       "y_rows": "tma-staged" if a.ystage else "per-thread loads"}},
             "fp64": out_fp64,
             "fp32_over_fp64": (v32 / out_fp64["value"]) if out_fp64 else None,
             "rho_rel_l1_fp32_vs_fp64": l1,

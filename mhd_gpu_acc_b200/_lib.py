@@ -95,7 +95,7 @@ PROTOTYPES = {
     "mhd_get_ch": (_I, [_P, _pd]),
     "mhd_set_limiter": (_I, [_P, _I]),
     "mhd_set_cr": (_I, [_P, _D]),
-    "mhd_set_sweep_shape": (_I, [_P, _I, _I]),
+    "mhd_set_sweep_shape": (_I, [_P, _I, _I, _I]),
     "mhd_compute_dt": (_I, [_P, _pg, _D, _pd]),
     "mhd_advance": (_I, [_P, _pg, _pg, _pg, _D, _I, _pi]),
     "mhd_apply_boundary": (_I, [_P, _pg, _pi]),

@@ -1,4 +1,10 @@
-// aux_kernels.cu -- boundary conditions, precision conversion, diagnostics.
+// aux_kernels.cu -- boundary conditions, precision conversion, diagnostics,
+// and the tensor maps of the TMA-staged sweep.
+#include <cuda.h>
+
+#include <cstdint>
+#include <mutex>
+
 #include "launch.h"
 #include "sweep.cuh"
 
@@ -247,6 +253,41 @@ cudaError_t launch_diagnostics(const DevGrid& g, int elem_bytes, double gamma, d
 cudaError_t launch_clock_init(DevClock* c, const unsigned long long* max0, cudaStream_t st) {
     clock_init_kernel<<<1, 1, 0, st>>>(c, max0);
     return cudaGetLastError();
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links only the CUDA runtime).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+bool rows_tensor_map(void* map64, const DevGrid& g, int elem_bytes, int box_cols, int box_rows) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || (reinterpret_cast<std::uintptr_t>(g.data) % 16) || ((g.pitch * elem_bytes) % 16) ||
+        ((g.plane * elem_bytes) % 16))
+        return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)g.tnx(), (cuuint64_t)g.tny(), (cuuint64_t)NV};
+    const cuuint64_t strides[2] = {(cuuint64_t)(g.pitch * elem_bytes), (cuuint64_t)(g.plane * elem_bytes)};
+    const cuuint32_t box[3] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows, (cuuint32_t)NV};
+    const cuuint32_t step[3] = {1, 1, 1};
+    return fn(static_cast<CUtensorMap*>(map64),
+              elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, g.data, dims,
+              strides, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 }  // namespace mhd

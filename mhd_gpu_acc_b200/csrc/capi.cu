@@ -99,23 +99,37 @@ struct mhd_workspace {
     int limiter = MHD_LIMITER_MINMOD;
     int yseg = mhd::kDefaultYBand;  // y-sweep rows per warp band
     int xrpw = mhd::kDefaultXRpw;  // x-sweep rows per warp
+    int ystage = 0;                // y-sweep rows loaded per thread (1: staged by TMA)
     int nsm = 148;
     cudaStream_t stream = nullptr;
     unsigned long long* d_max = nullptr;
     mhd::DevClock* d_clock = nullptr;
+    int* d_fault = nullptr;       // ClockStatus bits from bounded device waits
     double* d_diag = nullptr;     // 6 * 1024 partials + 6 results
     void* d_stage = nullptr;      // FP64 staging for uploads/downloads
     size_t stage_bytes = 0;
     // graph of two captured steps
     cudaGraphExec_t graph = nullptr;
     struct Key {
-        void* u; void* t; int solver, limiter, bc[4], yseg, xrpw;
+        void* u; void* t; int solver, limiter, bc[4], yseg, xrpw, ystage, pad_;
         double gamma, cr, cfl, t_end;
         bool operator==(const Key& o) const { return std::memcmp(this, &o, sizeof(Key)) == 0; }
     } key{};
 };
 
 namespace {
+
+// Reads (and clears) the fault word after the stream has drained: a bounded
+// device wait that gave up turns into MHD_ERR_TIMEOUT.
+int check_fault(mhd_workspace* ws, const char* what) {
+    int f = 0;
+    if (cudaMemcpyAsync(&f, ws->d_fault, sizeof f, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ws->stream) != cudaSuccess)
+        return fail(MHD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(cudaGetLastError()));
+    if (f == 0) return MHD_OK;
+    cudaMemsetAsync(ws->d_fault, 0, sizeof(int), ws->stream);
+    return fail(MHD_ERR_TIMEOUT, "%s: a bounded wait for a staged tile gave up (status %d)", what, f);
+}
 
 int ensure_stage(mhd_workspace* ws, size_t bytes) {
     if (ws->stage_bytes >= bytes) return MHD_OK;
@@ -149,15 +163,16 @@ mhd::StepParams base_params(const mhd_workspace* ws, const mhd_grid* g, int solv
     for (int k = 0; k < 4; ++k) P.bc[k] = bc[k];
     P.any_dirichlet = (bc[0] == MHD_BC_DIRICHLET || bc[1] == MHD_BC_DIRICHLET || bc[2] == MHD_BC_DIRICHLET ||
                        bc[3] == MHD_BC_DIRICHLET);
+    P.fault = ws->d_fault;
     return P;
 }
 
 cudaError_t launch_step(const mhd_grid* g, const mhd::DevGrid& in, const mhd::DevGrid& tmp, const mhd::DevGrid& out,
                         const mhd::StepParams& P, cudaStream_t st, int yseg, int which = 3,
-                        int xrpw = mhd::kDefaultXRpw) {
+                        int xrpw = mhd::kDefaultXRpw, int ystage = 0) {
     g_launches += (which == 3) ? 2 : 1;
-    return g->dtype == MHD_F64 ? mhd::launch_step_f64(in, tmp, out, P, st, yseg, which, xrpw)
-                               : mhd::launch_step_f32(in, tmp, out, P, st, yseg, which, xrpw);
+    return g->dtype == MHD_F64 ? mhd::launch_step_f64(in, tmp, out, P, st, yseg, which, xrpw, ystage)
+                               : mhd::launch_step_f32(in, tmp, out, P, st, yseg, which, xrpw, ystage);
 }
 
 cudaError_t launch_max(const mhd_workspace* ws, const mhd_grid* g, cudaStream_t st) {
@@ -345,11 +360,13 @@ int mhd_workspace_create(const mhd_grid* g, mhd_workspace** out) {
     if (ws->nsm <= 0) ws->nsm = 148;
     if (cudaMalloc(&ws->d_max, sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc(&ws->d_clock, sizeof(mhd::DevClock)) != cudaSuccess ||
+        cudaMalloc(&ws->d_fault, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ws->d_diag, sizeof(double) * (6 * 1024 + 8)) != cudaSuccess) {
         mhd_workspace_destroy(ws);
         return fail(MHD_ERR_NOMEM, "mhd_workspace_create: device scratch");
     }
     cudaMemset(ws->d_clock, 0, sizeof(mhd::DevClock));
+    cudaMemset(ws->d_fault, 0, sizeof(int));
     *out = ws;
     return MHD_OK;
 }
@@ -359,6 +376,7 @@ int mhd_workspace_destroy(mhd_workspace* ws) {
     if (ws->graph) cudaGraphExecDestroy(ws->graph);
     if (ws->d_max) cudaFree(ws->d_max);
     if (ws->d_clock) cudaFree(ws->d_clock);
+    if (ws->d_fault) cudaFree(ws->d_fault);
     if (ws->d_diag) cudaFree(ws->d_diag);
     if (ws->d_stage) cudaFree(ws->d_stage);
     delete ws;
@@ -409,12 +427,13 @@ int mhd_set_cr(mhd_workspace* ws, double cr) {
     return MHD_OK;
 }
 
-int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband) {
+int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage) {
     if (!ws) return fail(MHD_ERR_STATE, "mhd_set_sweep_shape: null workspace");
-    if (xrpw < 1 || xrpw > 64 || yband < 1 || yband > 65536)
-        return fail(MHD_ERR_ARG, "mhd_set_sweep_shape: need 1 <= xrpw <= 64 and 1 <= yband <= 65536");
+    if (xrpw < 1 || xrpw > 64 || yband < 1 || yband > 65536 || ystage < 0 || ystage > 1)
+        return fail(MHD_ERR_ARG, "mhd_set_sweep_shape: need 1 <= xrpw <= 64, 1 <= yband <= 65536, ystage 0 or 1");
     ws->xrpw = xrpw;
     ws->yseg = yband;
+    ws->ystage = ystage;
     return MHD_OK;
 }
 
@@ -426,7 +445,8 @@ int mhd_compute_dt(mhd_workspace* ws, const mhd_grid* g, double cfl, double* dt)
     CK(launch_max(ws, g, ws->stream));
     unsigned long long bits = 0;
     CK(cudaMemcpyAsync(&bits, ws->d_max, sizeof bits, cudaMemcpyDeviceToHost, ws->stream));
-    CK(cudaStreamSynchronize(ws->stream));
+    rc = check_fault(ws, "mhd_compute_dt");  // synchronises the stream
+    if (rc) return rc;
     double mx;
     std::memcpy(&mx, &bits, sizeof mx);
     if (!(mx > 0.0)) {
@@ -458,7 +478,7 @@ int mhd_advance(mhd_workspace* ws, const mhd_grid* Uold, mhd_grid* Utmp, mhd_gri
     if (P.damp >= 1.0) P.damp = 1.0;
     P.t_end = 0.0;
     P.cfl = 0.0;
-    CK(launch_step(Uold, dev(Uold), dev(Utmp), dev(Unew), P, ws->stream, ws->yseg, 3, ws->xrpw));
+    CK(launch_step(Uold, dev(Uold), dev(Utmp), dev(Unew), P, ws->stream, ws->yseg, 3, ws->xrpw, ws->ystage));
     return MHD_OK;
 }
 
@@ -513,9 +533,9 @@ int mhd_profile_sweeps(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, 
         mhd::StepParams Q = P;
         Q.parity = r & 1;
         cudaEventRecord(ev[0], st);
-        e = launch_step(U, dU, dT, dU, Q, st, ws->yseg, 1, ws->xrpw);
+        e = launch_step(U, dU, dT, dU, Q, st, ws->yseg, 1, ws->xrpw, ws->ystage);
         cudaEventRecord(ev[1], st);
-        if (e == cudaSuccess) e = launch_step(U, dU, dT, dU, Q, st, ws->yseg, 2);
+        if (e == cudaSuccess) e = launch_step(U, dU, dT, dU, Q, st, ws->yseg, 2, ws->xrpw, ws->ystage);
         cudaEventRecord(ev[2], st);
         if (e == cudaSuccess) e = cudaEventSynchronize(ev[2]);
         float a = 0.f, b = 0.f;
@@ -528,7 +548,7 @@ int mhd_profile_sweeps(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, 
     if (e != cudaSuccess) return fail(MHD_ERR_CUDA, "mhd_profile_sweeps: %s", cudaGetErrorString(e));
     ms_out[0] = sx / nrep;
     ms_out[1] = sy / nrep;
-    return MHD_OK;
+    return check_fault(ws, "mhd_profile_sweeps");
 }
 
 int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_end, int max_steps, int solver,
@@ -541,7 +561,7 @@ int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_en
     mhd_workspace::Key key{};
     key.u = U->data; key.t = T->data; key.solver = solver; key.limiter = ws->limiter;
     for (int k = 0; k < 4; ++k) key.bc[k] = bc[k];
-    key.yseg = ws->yseg; key.xrpw = ws->xrpw; key.gamma = ws->gamma; key.cr = ws->cr; key.cfl = cfl; key.t_end = t_end;
+    key.yseg = ws->yseg; key.xrpw = ws->xrpw; key.ystage = ws->ystage; key.gamma = ws->gamma; key.cr = ws->cr; key.cfl = cfl; key.t_end = t_end;
     const mhd::DevGrid dU = dev(U), dT = dev(T);
     if (!ws->graph || !(ws->key == key)) {
         if (ws->graph) { cudaGraphExecDestroy(ws->graph); ws->graph = nullptr; }
@@ -552,13 +572,15 @@ int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_en
             own = true;
         }
         cudaGraph_t gr = nullptr;
+        // one-time kernel attribute setup happens outside the capture
+        CK(launch_step(U, dU, dT, dU, P, cap, ws->yseg, 0, ws->xrpw, ws->ystage));
         CK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
         cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
         for (int par = 0; par < 2 && e1 == cudaSuccess; ++par) {
             mhd::StepParams Q = P;
             Q.parity = par;
-            e1 = (U->dtype == MHD_F64) ? mhd::launch_step_f64(dU, dT, dU, Q, cap, ws->yseg, 3, ws->xrpw)
-                                       : mhd::launch_step_f32(dU, dT, dU, Q, cap, ws->yseg, 3, ws->xrpw);
+            e1 = (U->dtype == MHD_F64) ? mhd::launch_step_f64(dU, dT, dU, Q, cap, ws->yseg, 3, ws->xrpw, ws->ystage)
+                                       : mhd::launch_step_f32(dU, dT, dU, Q, cap, ws->yseg, 3, ws->xrpw, ws->ystage);
         }
         e2 = cudaStreamEndCapture(cap, &gr);
         if (own) cudaStreamDestroy(cap);
@@ -582,7 +604,7 @@ int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_en
         if (max_steps & 1) {
             mhd::StepParams Q = P;
             Q.parity = 0;
-            CK(launch_step(U, dU, dT, dU, Q, st, ws->yseg, 3, ws->xrpw));
+            CK(launch_step(U, dU, dT, dU, Q, st, ws->yseg, 3, ws->xrpw, ws->ystage));
         }
         CK(cudaMemcpyAsync(&hc, ws->d_clock, sizeof hc, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -608,6 +630,8 @@ int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_en
         info->fallbacks = hc.flux_fallbacks;
         info->pad_ = 0;
     }
+    const int frc = check_fault(ws, "mhd_run");
+    if (frc) return frc;
     const int code = status_code(hc.status);
     if (code != MHD_OK) return fail(code, "mhd_run: step loop stopped with status %d after %d steps", hc.status, hc.steps);
     return MHD_OK;
@@ -662,7 +686,7 @@ int mhd_initialise_orszag_tang(mhd_workspace* ws, const mhd_grid* g, double b0, 
 int mhd_synchronize(mhd_workspace* ws) {
     if (!ws) return fail(MHD_ERR_STATE, "mhd_synchronize: null workspace");
     CK(cudaStreamSynchronize(ws->stream));
-    return MHD_OK;
+    return check_fault(ws, "mhd_synchronize");
 }
 
 int mhd_diagnostics(mhd_workspace* ws, const mhd_grid* g, double* out6) {

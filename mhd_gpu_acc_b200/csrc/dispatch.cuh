@@ -5,13 +5,34 @@
 // per warp.
 #pragma once
 
-#include "sweep.cuh"
+#include "launch.h"
+#include "sweep_tma.cuh"
 
 namespace mhd {
 
+// Dynamic shared memory opt-in of the TMA y-sweep, once per policy, with the
+// shared-memory carveout at its maximum so that kYBlocks CTAs' rings fit on an SM.
+template <class PH>
+cudaError_t y_tma_setup() {
+    static const cudaError_t e = [] {
+        cudaError_t r = cudaFuncSetAttribute(sweep_y_tma_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             yt_smem_bytes<typename PH::Real>());
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(sweep_y_tma_kernel<PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+        return r;
+    }();
+    return e;
+}
+
 template <class PH>
 cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                          cudaStream_t st, int yband, int which, int xrpw) {
+                          cudaStream_t st, int yband, int which, int xrpw, int ystage) {
+    using R = typename PH::Real;
+    if (ystage == 1) {
+        const cudaError_t e = y_tma_setup<PH>();
+        if (e != cudaSuccess) return e;
+    }
     if (which & 1) {
         const int rows_per_cta = XS_ROWS * xrpw;
         const dim3 bx(32 * XS_ROWS), gx((in.nx + XS_TX - 1) / XS_TX, (in.ny + rows_per_cta - 1) / rows_per_cta);
@@ -19,9 +40,18 @@ cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
     }
     if (which & 2) {
         const int per = yband > 0 ? yband : kDefaultYBand;
-        const long long warps = (long long)y_strips(tmp) * ((tmp.ny + per - 1) / per);
-        const unsigned grid = (unsigned)((warps + YS_WARPS - 1) / YS_WARPS);
-        sweep_y_kernel<PH><<<grid, dim3(32, YS_WARPS), 0, st>>>(tmp, out, P, per);
+        const long long bands = (tmp.ny + per - 1) / per;
+        alignas(64) CUtensorMap map;
+        if (ystage == 1 && P.fault &&
+            rows_tensor_map(&map, tmp, (int)sizeof(R), YT_COLS, YTShape<R>::ROWS)) {
+            const long long groups = (y_strips(tmp) + YT_WARPS - 1) / YT_WARPS;
+            sweep_y_tma_kernel<PH><<<(unsigned)(groups * bands), dim3(32, YT_WARPS), yt_smem_bytes<R>(), st>>>(
+                map, tmp, out, P, per);
+        } else {
+            const long long warps = (long long)y_strips(tmp) * bands;
+            const unsigned grid = (unsigned)((warps + YS_WARPS - 1) / YS_WARPS);
+            sweep_y_kernel<PH><<<grid, dim3(32, YS_WARPS), 0, st>>>(tmp, out, P, per);
+        }
     }
     return cudaGetLastError();
 }
@@ -46,15 +76,15 @@ struct StepLaunch {
     const DevGrid &in, &tmp, &out;
     const StepParams& P;
     cudaStream_t st;
-    int yseg, which, xrpw;
+    int yseg, which, xrpw, ystage;
     template <class PH>
-    cudaError_t run() const { return launch_policy<PH>(in, tmp, out, P, st, yseg, which, xrpw); }
+    cudaError_t run() const { return launch_policy<PH>(in, tmp, out, P, st, yseg, which, xrpw, ystage); }
 };
 
 template <template <int, int> class POL>
 cudaError_t dispatch_step(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                          cudaStream_t st, int yseg, int which, int xrpw) {
-    StepLaunch go{in, tmp, out, P, st, yseg, which, xrpw};
+                          cudaStream_t st, int yseg, int which, int xrpw, int ystage) {
+    StepLaunch go{in, tmp, out, P, st, yseg, which, xrpw, ystage};
     return with_policy<POL>(P.solver, P.limiter, go);
 }
 

@@ -9,11 +9,19 @@
 namespace mhd {
 
 // One split step Uin -> Utmp (x) -> Uout (y), reference semantics.
-// which: 1 = x-sweep only, 2 = y-sweep only, 3 = both.
+// which: 1 = x-sweep only, 2 = y-sweep only, 3 = both, 0 = nothing (only the
+// one-time kernel attribute setup, so that a later stream capture makes none).
+// ystage: 1 = y-sweep rows staged by TMA (needs P.fault and a 16-byte aligned
+// slab; other grids use per-thread loads), 0 = per-thread loads.
 cudaError_t launch_step_f64(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                            cudaStream_t st, int yseg, int which = 3, int xrpw = kDefaultXRpw);
+                            cudaStream_t st, int yseg, int which = 3, int xrpw = kDefaultXRpw, int ystage = 0);
 cudaError_t launch_step_f32(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                            cudaStream_t st, int yseg, int which = 3, int xrpw = kDefaultXRpw);
+                            cudaStream_t st, int yseg, int which = 3, int xrpw = kDefaultXRpw, int ystage = 0);
+
+// 3D tensor map (x, row, field) over the 9 planes of `g` with boxes of
+// box_cols x box_rows x 9; false when the slab is not TMA-addressable (base or
+// strides not 16-byte multiples) or the driver has no encoder.
+bool rows_tensor_map(void* map64, const DevGrid& g, int elem_bytes, int box_cols, int box_rows);
 
 // Batched instances: one persistent launch per sweep over the global work list
 // (batch.cuh).  which = 1: x-sweeps of every instance, 2: y-sweeps.

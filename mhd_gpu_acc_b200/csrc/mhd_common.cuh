@@ -84,6 +84,7 @@ struct StepParams {
     int any_dirichlet;
     int accumulate;   // y-sweep: also fold the next max signal speed into maxbits
     unsigned long long* max_out;  // explicit mode accumulation target (may be null)
+    int* fault;       // ClockStatus bits of a bounded device wait that gave up (may be null)
 };
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

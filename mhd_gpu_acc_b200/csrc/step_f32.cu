@@ -36,8 +36,8 @@ struct FastPolicy {
 };
 
 cudaError_t launch_step_f32(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                            cudaStream_t st, int yseg, int which, int xrpw) {
-    return dispatch_step<FastPolicy>(in, tmp, out, P, st, yseg, which, xrpw);
+                            cudaStream_t st, int yseg, int which, int xrpw, int ystage) {
+    return dispatch_step<FastPolicy>(in, tmp, out, P, st, yseg, which, xrpw, ystage);
 }
 
 cudaError_t launch_batch_f32(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,

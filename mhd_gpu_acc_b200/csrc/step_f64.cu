@@ -37,8 +37,8 @@ struct ExactPolicy {
 };
 
 cudaError_t launch_step_f64(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
-                            cudaStream_t st, int yseg, int which, int xrpw) {
-    return dispatch_step<ExactPolicy>(in, tmp, out, P, st, yseg, which, xrpw);
+                            cudaStream_t st, int yseg, int which, int xrpw, int ystage) {
+    return dispatch_step<ExactPolicy>(in, tmp, out, P, st, yseg, which, xrpw, ystage);
 }
 
 cudaError_t launch_batch_f64(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,
