@@ -115,6 +115,11 @@ int mhd_set_cr(mhd_workspace* ws, double cr);
  * (same results; on B200 at 4096^2 FP32 the staged sweep measured 0.81 ms
  * against 0.72 ms). */
 int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage);
+/* Cell spacing the step and compute_dt use instead of the grid's
+ * (x_max - x_min) / nx and (y_max - y_min) / ny; (0, 0) restores those.  A slab
+ * of a larger grid takes the global spacing, so that its steps equal the
+ * unsplit grid's bit for bit (no counterpart in the reference). */
+int mhd_set_spacing(mhd_workspace* ws, double dx, double dy);
 
 /* Replaces compute_dt_gpu (src/gpu/solver_gpu.cu:578-605): CFL maximum over the
  * interior floored by the current ch; sets ch to it and returns
@@ -127,6 +132,20 @@ int mhd_compute_dt(mhd_workspace* ws, const mhd_grid* g, double cfl, double* dt)
  * psi damping -- one fused kernel per sweep.  bc = {left, right, bottom, top}. */
 int mhd_advance(mhd_workspace* ws, const mhd_grid* Uold, mhd_grid* Utmp, mhd_grid* Unew, double dt, int solver,
                 const int* bc);
+
+/* One sweep of mhd_advance (no reference counterpart): dir 0 = the x-sweep
+ * in -> out, dir 1 = the y-sweep in -> out with the psi damping, each with its
+ * boundary fill, at dt and the workspace's ch.  mhd_advance is the x-sweep
+ * followed by the y-sweep; between them a caller may rewrite ghost rows of the
+ * x-swept state (the halo exchange of a grid split into y-slabs). */
+int mhd_sweep(mhd_workspace* ws, const mhd_grid* in, mhd_grid* out, double dt, int solver, const int* bc, int dir);
+/* The CFL maximum of mhd_compute_dt (interior, floored by the current ch)
+ * without changing ch or forming dt: the per-slab term of a global maximum. */
+int mhd_max_speed(mhd_workspace* ws, const mhd_grid* g, double* vmax);
+/* Copies nrows full storage rows (ghost columns included) of all 9 fields,
+ * src rows [src_row, src_row + nrows) -> dst rows [dst_row, ...), between grids
+ * of equal nx, ng, dtype and pitch, asynchronously on `stream`. */
+int mhd_grid_copy_rows(const mhd_grid* src, int src_row, mhd_grid* dst, int dst_row, int nrows, void* stream);
 
 /* Replaces apply_boundary_gpu (src/gpu/boundary_gpu.cu:158-176), in place. */
 int mhd_apply_boundary(mhd_workspace* ws, mhd_grid* g, const int* bc);

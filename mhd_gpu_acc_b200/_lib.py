@@ -96,9 +96,13 @@ PROTOTYPES = {
     "mhd_set_limiter": (_I, [_P, _I]),
     "mhd_set_cr": (_I, [_P, _D]),
     "mhd_set_sweep_shape": (_I, [_P, _I, _I, _I]),
+    "mhd_set_spacing": (_I, [_P, _D, _D]),
     "mhd_compute_dt": (_I, [_P, _pg, _D, _pd]),
     "mhd_advance": (_I, [_P, _pg, _pg, _pg, _D, _I, _pi]),
     "mhd_apply_boundary": (_I, [_P, _pg, _pi]),
+    "mhd_sweep": (_I, [_P, _pg, _pg, _D, _I, _pi, _I]),
+    "mhd_max_speed": (_I, [_P, _pg, _pd]),
+    "mhd_grid_copy_rows": (_I, [_pg, _I, _pg, _I, _I, _P]),
     "mhd_advance_noalloc": (_I, [_pg, _pg, _D, _D, _D, _D, _I, _I, _pi, _P]),
     "mhd_run": (_I, [_P, _pg, _pg, _D, _D, _I, _I, _pi, C.POINTER(mhd_run_info)]),
     "mhd_profile_sweeps": (_I, [_P, _pg, _pg, _D, _D, _I, _pi, _I, C.POINTER(C.c_float)]),

@@ -100,6 +100,7 @@ struct mhd_workspace {
     int yseg = mhd::kDefaultYBand;  // y-sweep rows per warp band
     int xrpw = mhd::kDefaultXRpw;  // x-sweep rows per warp
     int ystage = 0;                // y-sweep rows loaded per thread (1: staged by TMA)
+    double dx = 0.0, dy = 0.0;     // cell spacing of the step; 0 = from the grid's extent
     int nsm = 148;
     cudaStream_t stream = nullptr;
     unsigned long long* d_max = nullptr;
@@ -155,8 +156,8 @@ mhd::StepParams base_params(const mhd_workspace* ws, const mhd_grid* g, int solv
     std::memset(&P, 0, sizeof P);
     P.gamma = ws->gamma;
     P.cr = ws->cr;
-    P.dx = gdx(g);
-    P.dy = gdy(g);
+    P.dx = ws->dx > 0.0 ? ws->dx : gdx(g);
+    P.dy = ws->dy > 0.0 ? ws->dy : gdy(g);
     P.dmin = (P.dy < P.dx) ? P.dy : P.dx;
     P.solver = solver;
     P.limiter = ws->limiter;
@@ -437,6 +438,15 @@ int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage) {
     return MHD_OK;
 }
 
+int mhd_set_spacing(mhd_workspace* ws, double dx, double dy) {
+    if (!ws) return fail(MHD_ERR_STATE, "mhd_set_spacing: null workspace");
+    if (!(dx >= 0.0) || !(dy >= 0.0) || (dx > 0.0) != (dy > 0.0))
+        return fail(MHD_ERR_ARG, "mhd_set_spacing: need dx, dy > 0 (or both 0)");
+    ws->dx = dx;
+    ws->dy = dy;
+    return MHD_OK;
+}
+
 int mhd_compute_dt(mhd_workspace* ws, const mhd_grid* g, double cfl, double* dt) {
     int rc = check_ws_grid(ws, g, "mhd_compute_dt");
     if (rc) return rc;
@@ -454,7 +464,7 @@ int mhd_compute_dt(mhd_workspace* ws, const mhd_grid* g, double cfl, double* dt)
         return fail(MHD_ERR_NO_SPEED, "mhd_compute_dt: non-positive maximum wave speed");
     }
     ws->ch = mx;
-    const double dx = gdx(g), dy = gdy(g);
+    const double dx = ws->dx > 0.0 ? ws->dx : gdx(g), dy = ws->dy > 0.0 ? ws->dy : gdy(g);
     *dt = cfl * ((dy < dx) ? dy : dx) / mx;
     return MHD_OK;
 }
@@ -479,6 +489,61 @@ int mhd_advance(mhd_workspace* ws, const mhd_grid* Uold, mhd_grid* Utmp, mhd_gri
     P.t_end = 0.0;
     P.cfl = 0.0;
     CK(launch_step(Uold, dev(Uold), dev(Utmp), dev(Unew), P, ws->stream, ws->yseg, 3, ws->xrpw, ws->ystage));
+    return MHD_OK;
+}
+
+int mhd_sweep(mhd_workspace* ws, const mhd_grid* in, mhd_grid* out, double dt, int solver, const int* bc, int dir) {
+    int rc = check_ws_grid(ws, in, "mhd_sweep(in)");
+    if (!rc) rc = check_ws_grid(ws, out, "mhd_sweep(out)");
+    if (!rc) rc = check_bc(bc);
+    if (rc) return rc;
+    if (solver < MHD_HLL || solver > MHD_FORCE) return fail(MHD_ERR_ARG, "mhd_sweep: bad solver %d", solver);
+    if (dir != 0 && dir != 1) return fail(MHD_ERR_ARG, "mhd_sweep: dir must be 0 (x) or 1 (y)");
+    if (in->data == out->data) return fail(MHD_ERR_ARG, "mhd_sweep: in and out must be distinct");
+    mhd::StepParams P = base_params(ws, in, solver, bc);
+    P.dt = dt;
+    P.ch = ws->ch;
+    P.damp = std::exp(-dt * ws->ch / ws->cr);  // as mhd_advance
+    if (P.damp >= 1.0) P.damp = 1.0;
+    P.t_end = 0.0;
+    P.cfl = 0.0;
+    if (dir == 0) CK(launch_step(in, dev(in), dev(out), dev(out), P, ws->stream, ws->yseg, 1, ws->xrpw, ws->ystage));
+    else CK(launch_step(in, dev(in), dev(in), dev(out), P, ws->stream, ws->yseg, 2, ws->xrpw, ws->ystage));
+    return MHD_OK;
+}
+
+int mhd_max_speed(mhd_workspace* ws, const mhd_grid* g, double* vmax) {
+    int rc = check_ws_grid(ws, g, "mhd_max_speed");
+    if (rc) return rc;
+    if (!vmax) return fail(MHD_ERR_ARG, "mhd_max_speed: null output");
+    CK(cudaMemsetAsync(ws->d_max, 0, sizeof(unsigned long long), ws->stream));
+    CK(launch_max(ws, g, ws->stream));
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, ws->d_max, sizeof bits, cudaMemcpyDeviceToHost, ws->stream));
+    rc = check_fault(ws, "mhd_max_speed");  // synchronises the stream
+    if (rc) return rc;
+    std::memcpy(vmax, &bits, sizeof *vmax);
+    if (!(*vmax > 0.0)) return fail(MHD_ERR_NO_SPEED, "mhd_max_speed: non-positive maximum wave speed");
+    return MHD_OK;
+}
+
+int mhd_grid_copy_rows(const mhd_grid* src, int src_row, mhd_grid* dst, int dst_row, int nrows, void* stream) {
+    int rc = check_grid(src, "mhd_grid_copy_rows(src)");
+    if (!rc) rc = check_grid(dst, "mhd_grid_copy_rows(dst)");
+    if (rc) return rc;
+    if (src->nx != dst->nx || src->ng != dst->ng || src->dtype != dst->dtype || src->pitch != dst->pitch)
+        return fail(MHD_ERR_ARG, "mhd_grid_copy_rows: grids differ in nx, ng, dtype or pitch");
+    const int sty = src->ny + 2 * src->ng, dty = dst->ny + 2 * dst->ng;
+    if (nrows < 0 || src_row < 0 || dst_row < 0 || src_row + nrows > sty || dst_row + nrows > dty)
+        return fail(MHD_ERR_ARG, "mhd_grid_copy_rows: rows out of range");
+    const size_t e = elem_bytes(src->dtype);
+    const size_t bytes = (size_t)nrows * (size_t)src->pitch * e;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (int f = 0; f < MHD_NV; ++f) {
+        const char* s = static_cast<const char*>(src->data) + ((size_t)f * src->plane + (size_t)src_row * src->pitch) * e;
+        char* d = static_cast<char*>(dst->data) + ((size_t)f * dst->plane + (size_t)dst_row * dst->pitch) * e;
+        CK(cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToDevice, st));
+    }
     return MHD_OK;
 }
 

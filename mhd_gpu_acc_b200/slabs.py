@@ -1,0 +1,303 @@
+"""One grid split into y-slabs: the multi-GPU decomposition of a single large
+grid (one slab per GPU), and the same decomposition on one device.
+
+A step of the split scheme needs, between its two sweeps, the two x-swept rows
+on each side of a slab boundary: the y-sweep of row j reads rows j-2 .. j+1.
+The x-sweep is row-local and the CFL maximum is a max over cells, so a step on
+P slabs is
+    M = max over slabs of mhd_max_speed       (all-reduce(max) across ranks)
+    ch = M; dt = cfl * min(dx, dy) / M         (identical on every slab)
+    x-sweep of every slab (mhd_sweep, dir 0)
+    halo exchange: each slab's two first / last interior rows of the x-swept
+                   state -> the neighbour's ghost rows (2 x 9 rows per side)
+    y-sweep of every slab (mhd_sweep, dir 1)
+A side between two slabs is declared Dirichlet to the kernels: they then copy
+(not compute) its ghost rows, which the exchange overwrites before the y-sweep
+reads them, and no kernel reads a state's y-ghost rows otherwise.  The global
+y boundaries keep their own type; with periodic y the slabs form a ring.
+
+`SlabGrid` keeps all slabs on the current device (copies through
+mhd_grid_copy_rows) and is bit-identical to the single-grid step (every slab
+workspace steps with the global spacing, mhd_set_spacing).  `DistSlabRun`
+holds one slab per rank; its exchange, `exchange_rows`, sends the same rows
+with torch.distributed point-to-point operations (NCCL on GPUs, gloo on CPU).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from ._lib import check, load, mhd_grid
+from .solver import F64, BoundaryConfig, BoundaryType, GpuWorkspace, Grid2DGPU, init_gpu_workspace
+
+HALO = 2  # x-swept rows the y-sweep reads beyond a slab edge
+EXCHANGED = int(BoundaryType.Dirichlet)  # kernel boundary type of a side filled by the exchange
+
+
+def slab_rows(ny: int, parts: int) -> list[tuple[int, int]]:
+    """Interior row ranges [r0, r1) of `parts` slabs, sizes differing by at most one."""
+    if parts < 1 or parts > ny // HALO:
+        raise ValueError(f"cannot split {ny} rows into {parts} slabs of >= {HALO} rows")
+    base, extra = divmod(ny, parts)
+    out, r0 = [], 0
+    for p in range(parts):
+        r1 = r0 + base + (1 if p < extra else 0)
+        out.append((r0, r1))
+        r0 = r1
+    return out
+
+
+def neighbours(p: int, parts: int, periodic_y: bool) -> tuple[int | None, int | None]:
+    """(slab below, slab above) of slab p; None at a non-periodic global edge."""
+    below = p - 1 if p > 0 else (parts - 1 if periodic_y and parts > 1 else None)
+    above = p + 1 if p < parts - 1 else (0 if periodic_y and parts > 1 else None)
+    return below, above
+
+
+def slab_bc(bc, p: int, parts: int) -> tuple[int, int, int, int]:
+    """Boundary types handed to the kernels for slab p: the global left/right, and
+    the global bottom/top only on the outer slabs of a non-periodic y direction;
+    sides that receive an exchange are Dirichlet (ghost rows copied, then overwritten)."""
+    b = BoundaryConfig.of(bc)
+    periodic_y = int(b.bottom) == 0 and int(b.top) == 0
+    below, above = neighbours(p, parts, periodic_y)
+    if parts == 1:
+        return (int(b.left), int(b.right), int(b.bottom), int(b.top))
+    return (int(b.left), int(b.right), EXCHANGED if below is not None else int(b.bottom),
+            EXCHANGED if above is not None else int(b.top))
+
+
+def slab_extent(y_min: float, y_max: float, ny: int, r0: int, r1: int) -> tuple[float, float]:
+    """y extent of slab rows [r0, r1) of the global grid.  The slab's workspace
+    is also given the global spacing (mhd_set_spacing), because
+    (y1 - y0) / (r1 - r0) need not round back to the global dy."""
+    dy = (y_max - y_min) / ny
+    return y_min + r0 * dy, y_min + r1 * dy
+
+
+def halo_copies(rows, ng: int, periodic_y: bool):
+    """(src slab, src storage row, dst slab, dst storage row) of every 2-row block
+    of the exchange: slab p's top interior rows go to the bottom ghost rows of the
+    slab above, its bottom interior rows to the top ghost rows of the slab below."""
+    parts = len(rows)
+    out = []
+    for p, (r0, r1) in enumerate(rows):
+        n = r1 - r0
+        below, above = neighbours(p, parts, periodic_y)
+        if above is not None:
+            out.append((p, ng + n - HALO, above, ng - HALO))
+        if below is not None:
+            nb = rows[below][1] - rows[below][0]
+            out.append((p, ng, below, ng + nb))
+    return out
+
+
+class SlabGrid:
+    """A grid of nx x ny cells held as `parts` y-slabs on the current device."""
+
+    def __init__(self, nx: int, ny: int, ng: int, extent, parts: int, dtype: int = F64):
+        self.nx, self.ny, self.ng, self.parts, self.dtype = nx, ny, ng, parts, dtype
+        self.extent = tuple(float(v) for v in extent)
+        x0, x1, y0, y1 = self.extent
+        self.rows = slab_rows(ny, parts)
+        self.U, self.T, self.N, self.ws = [], [], [], []
+        for r0, r1 in self.rows:
+            e = (x0, x1) + slab_extent(y0, y1, ny, r0, r1)
+            U = Grid2DGPU(nx, r1 - r0, ng, *e, dtype)
+            self.U.append(U)
+            self.T.append(Grid2DGPU(nx, r1 - r0, ng, *e, dtype))
+            self.N.append(Grid2DGPU(nx, r1 - r0, ng, *e, dtype))
+            ws = GpuWorkspace()
+            init_gpu_workspace(ws, U)
+            check(load().mhd_set_spacing(ws.ptr, (x1 - x0) / nx, (y1 - y0) / ny), "mhd_set_spacing")
+            self.ws.append(ws)
+
+    def upload(self, host: np.ndarray) -> None:
+        """Global dense FP64 SoA (9, ny+2ng, nx+2ng) -> slabs (each with its ng ghost rows)."""
+        ng = self.ng
+        for (r0, r1), U, T, N in zip(self.rows, self.U, self.T, self.N):
+            part = np.ascontiguousarray(host[:, r0:r1 + 2 * ng, :])
+            for g in (U, T, N):
+                g.upload(part)
+
+    def download(self) -> np.ndarray:
+        """Slabs -> global array; the global ghost rows come from the outer slabs."""
+        ng = self.ng
+        out = np.empty((9, self.ny + 2 * ng, self.nx + 2 * ng))
+        for p, ((r0, r1), U) in enumerate(zip(self.rows, self.U)):
+            a = U.download()
+            lo = 0 if p == 0 else ng
+            hi = (r1 - r0 + 2 * ng) if p == self.parts - 1 else (r1 - r0 + ng)
+            out[:, r0 + lo:r0 + hi, :] = a[:, lo:hi, :]
+        return out
+
+    def configure(self, gamma: float, limiter: int, cr: float | None = None, ch: float = 0.0) -> None:
+        lib = load()
+        for ws in self.ws:
+            check(lib.mhd_set_gamma(ws.ptr, float(gamma)), "mhd_set_gamma")
+            check(lib.mhd_set_ch(ws.ptr, float(ch)), "mhd_set_ch")
+            ws.set_limiter(limiter)
+            if cr is not None:
+                ws.set_cr(cr)
+
+    def max_speed(self) -> float:
+        lib = load()
+        m = C.c_double()
+        best = 0.0
+        for ws, U in zip(self.ws, self.U):
+            check(lib.mhd_max_speed(ws.ptr, C.byref(U.g), C.byref(m)), "mhd_max_speed")
+            best = max(best, m.value)
+        return best
+
+    def step(self, cfl: float, solver: int, bc, t_left: float = math.inf) -> float:
+        """One split step of the whole grid; returns dt (clamped to t_left)."""
+        lib = load()
+        b = BoundaryConfig.of(bc)
+        periodic_y = int(b.bottom) == 0 and int(b.top) == 0
+        M = self.max_speed()
+        for ws in self.ws:
+            check(lib.mhd_set_ch(ws.ptr, M), "mhd_set_ch")
+        x0, x1, y0, y1 = self.extent
+        dx, dy = (x1 - x0) / self.nx, (y1 - y0) / self.ny
+        dt = cfl * (dy if dy < dx else dx) / M
+        dt = min(dt, t_left)
+        bcs = [(C.c_int * 4)(*slab_bc(b, p, self.parts)) for p in range(self.parts)]
+        for p in range(self.parts):
+            check(lib.mhd_sweep(self.ws[p].ptr, C.byref(self.U[p].g), C.byref(self.T[p].g), dt, int(solver), bcs[p], 0),
+                  "mhd_sweep(x)")
+        self.synchronize()
+        for s, sr, d, dr in halo_copies(self.rows, self.ng, periodic_y):
+            check(lib.mhd_grid_copy_rows(C.byref(self.T[s].g), sr, C.byref(self.T[d].g), dr, HALO, None),
+                  "mhd_grid_copy_rows")
+        check(lib.mhd_synchronize(self.ws[0].ptr), "mhd_synchronize")
+        for p in range(self.parts):
+            check(lib.mhd_sweep(self.ws[p].ptr, C.byref(self.T[p].g), C.byref(self.N[p].g), dt, int(solver), bcs[p], 1),
+                  "mhd_sweep(y)")
+        for p in range(self.parts):
+            self.U[p].swap(self.N[p])
+        self.synchronize()
+        return dt
+
+    def synchronize(self) -> None:
+        lib = load()
+        for ws in self.ws:
+            check(lib.mhd_synchronize(ws.ptr), "mhd_synchronize")
+
+    def destroy(self) -> None:
+        for ws in self.ws:
+            ws.destroy()
+        self.ws = []
+
+
+def exchange_rows(state, rows_here: int, ng: int, below: int | None, above: int | None, dist) -> None:
+    """Rank-to-rank halo exchange on a torch tensor `state` of shape
+    (9, rows_here + 2 ng, width) holding this rank's x-swept slab: sends the two
+    first / last interior rows to the ranks below / above and receives their rows
+    into the ghost rows, with torch.distributed point-to-point operations (the
+    collective steps are the same on every rank).  below / above are ranks or None.
+    Messages between two ranks match in posting order, so every rank posts
+    "send up, send down" and then "receive from below, receive from above": with
+    two ranks in a periodic ring (below == above) the first message is still the
+    sender's top rows, and it lands in the receiver's bottom ghost rows."""
+    import torch
+
+    ops, recv = [], []
+    if above is not None:
+        ops.append(dist.P2POp(dist.isend, state[:, ng + rows_here - HALO:ng + rows_here, :].contiguous(), above))
+    if below is not None:
+        ops.append(dist.P2POp(dist.isend, state[:, ng:ng + HALO, :].contiguous(), below))
+    if below is not None:
+        buf = torch.empty_like(state[:, :HALO, :])
+        ops.append(dist.P2POp(dist.irecv, buf, below))
+        recv.append((buf, ng - HALO))
+    if above is not None:
+        buf = torch.empty_like(state[:, :HALO, :])
+        ops.append(dist.P2POp(dist.irecv, buf, above))
+        recv.append((buf, ng + rows_here))
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+    for buf, r in recv:
+        state[:, r:r + HALO, :] = buf
+
+
+class _DeviceRows:
+    """__cuda_array_interface__ view (9, ny + 2 ng, pitch) of a grid's device slab."""
+
+    def __init__(self, g: mhd_grid):
+        tny = g.ny + 2 * g.ng
+        es = 8 if g.dtype == F64 else 4
+        self.__cuda_array_interface__ = {
+            "shape": (9, tny, int(g.pitch)), "typestr": "<f8" if es == 8 else "<f4",
+            "strides": (int(g.plane) * es, int(g.pitch) * es, es), "data": (int(g.data), False), "version": 3,
+        }
+
+
+def grid_tensor(g: mhd_grid):
+    """A torch tensor sharing the device memory of grid g (no copy)."""
+    import torch
+
+    return torch.as_tensor(_DeviceRows(g), device="cuda")
+
+
+class DistSlabRun:
+    """One slab per rank of a torch.distributed group (NCCL): the rank's rows of the
+    global grid, its halo exchange with `exchange_rows` and the CFL maximum with an
+    all-reduce(max).  Every rank calls step() the same number of times."""
+
+    def __init__(self, nx: int, ny: int, ng: int, extent, dtype: int = F64):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        self.nx, self.ny, self.ng = nx, ny, ng
+        self.extent = tuple(float(v) for v in extent)
+        self.rows = slab_rows(ny, self.world)
+        r0, r1 = self.rows[self.rank]
+        x0, x1, y0, y1 = self.extent
+        e = (x0, x1) + slab_extent(y0, y1, ny, r0, r1)
+        self.U = Grid2DGPU(nx, r1 - r0, ng, *e, dtype)
+        self.T = Grid2DGPU(nx, r1 - r0, ng, *e, dtype)
+        self.N = Grid2DGPU(nx, r1 - r0, ng, *e, dtype)
+        self.ws = GpuWorkspace()
+        init_gpu_workspace(self.ws, self.U)
+        self.dx, self.dy = (x1 - x0) / nx, (y1 - y0) / ny
+        check(load().mhd_set_spacing(self.ws.ptr, self.dx, self.dy), "mhd_set_spacing")
+
+    def upload(self, host: np.ndarray) -> None:
+        """This rank's rows (with ghost rows) of the global dense FP64 SoA array."""
+        r0, r1 = self.rows[self.rank]
+        part = np.ascontiguousarray(host[:, r0:r1 + 2 * self.ng, :])
+        for g in (self.U, self.T, self.N):
+            g.upload(part)
+
+    def step(self, cfl: float, solver: int, bc) -> float:
+        import torch
+
+        lib = load()
+        b = BoundaryConfig.of(bc)
+        periodic_y = int(b.bottom) == 0 and int(b.top) == 0
+        m = C.c_double()
+        check(lib.mhd_max_speed(self.ws.ptr, C.byref(self.U.g), C.byref(m)), "mhd_max_speed")
+        M = torch.tensor([m.value], dtype=torch.float64, device="cuda")
+        self.dist.all_reduce(M, op=self.dist.ReduceOp.MAX)
+        M = float(M.item())
+        check(lib.mhd_set_ch(self.ws.ptr, M), "mhd_set_ch")
+        dx, dy = self.dx, self.dy
+        dt = cfl * (dy if dy < dx else dx) / M
+        sbc = (C.c_int * 4)(*slab_bc(b, self.rank, self.world))
+        check(lib.mhd_sweep(self.ws.ptr, C.byref(self.U.g), C.byref(self.T.g), dt, int(solver), sbc, 0), "mhd_sweep(x)")
+        check(lib.mhd_synchronize(self.ws.ptr), "mhd_synchronize")
+        below, above = neighbours(self.rank, self.world, periodic_y)
+        r0, r1 = self.rows[self.rank]
+        exchange_rows(grid_tensor(self.T.g), r1 - r0, self.ng, below, above, self.dist)
+        torch.cuda.synchronize()
+        check(lib.mhd_sweep(self.ws.ptr, C.byref(self.T.g), C.byref(self.N.g), dt, int(solver), sbc, 1), "mhd_sweep(y)")
+        self.U.swap(self.N)
+        check(lib.mhd_synchronize(self.ws.ptr), "mhd_synchronize")
+        return dt
+
+    def destroy(self) -> None:
+        self.ws.destroy()

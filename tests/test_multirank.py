@@ -1,11 +1,13 @@
-"""Multi-rank host logic on CPU: LPT sharding of a batch over GPUs and the rank
-reductions bench.py times with, as two gloo ranks launched by
-torch.distributed.run (the N > 1 path of the bench without a GPU), plus the
-loss of a rank between steps."""
+"""Multi-rank host logic on CPU: LPT sharding of a batch over GPUs, the rank
+reductions bench.py times with, and the y-slab halo exchange of one grid split
+over ranks, as gloo ranks launched by torch.distributed.run (the N > 1 paths
+without a GPU), plus the loss of a rank between steps."""
 import os
 import socket
 import subprocess
 import sys
+
+import pytest
 
 from mhd_gpu_acc_b200.batch import lpt_partition, orszag_tang_batch_spec
 
@@ -32,9 +34,10 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _torchrun(mode: str):
+def _torchrun(mode: str, nproc: int = 2):
     cmd = ["timeout", "-k", "10", "150", sys.executable, "-m", "torch.distributed.run", "--nnodes", "1",
-           "--nproc-per-node", "2", "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), WORKER, mode]
+           "--nproc-per-node", str(nproc), "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), WORKER,
+           mode]
     env = dict(os.environ, CUDA_VISIBLE_DEVICES="", OMP_NUM_THREADS="1")
     return subprocess.run(cmd, capture_output=True, text=True, timeout=200, env=env, cwd=ROOT)
 
@@ -49,3 +52,11 @@ def test_lost_rank_is_detected_not_hung():
     r = _torchrun("fail")
     assert r.returncode != 0
     assert r.returncode != 124, "the surviving rank hung"
+
+
+@pytest.mark.parametrize("mode,nproc", [("halo", 2), ("halo", 3), ("halo_periodic", 2), ("halo_periodic", 3)])
+def test_slab_halo_exchange_between_ranks(mode, nproc):
+    """The y-slab exchange of one grid split over ranks (mhd_gpu_acc_b200.slabs.exchange_rows)."""
+    r = _torchrun(mode, nproc)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert all(f"rank {k} ok" in r.stdout for k in range(nproc))
