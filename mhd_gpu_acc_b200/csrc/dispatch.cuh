@@ -34,8 +34,8 @@ cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
         if (e != cudaSuccess) return e;
     }
     if (which & 1) {
-        const int rows_per_cta = XS_ROWS * xrpw;
-        const dim3 bx(32 * XS_ROWS), gx((in.nx + XS_TX - 1) / XS_TX, (in.ny + rows_per_cta - 1) / rows_per_cta);
+        const int rows_per_cta = PH::kXWarps * xrpw;
+        const dim3 bx(32 * PH::kXWarps), gx((in.nx + XS_TX - 1) / XS_TX, (in.ny + rows_per_cta - 1) / rows_per_cta);
         sweep_x_kernel<PH><<<gx, bx, 0, st>>>(in, tmp, P, xrpw);
     }
     if (which & 2) {

@@ -17,6 +17,11 @@ struct ExactPolicy {
     static constexpr int NW = NV;  // primitive values per cell
     static constexpr int NS = NV;  // values per reconstructed side state (U*)
     static constexpr int kYBlocks = 2;  // y-sweep CTAs per SM the register budget is cut for
+    // x-sweep: 4 warps per CTA, 3 CTAs per SM (168 registers, a few spilled).
+    // Measured at 4096^2 (HLLD, van Leer): 2.29 ms, against 2.65 ms for one CTA
+    // of 8 warps (240 registers) and 2.35 ms for 2 warps x 6.
+    static constexpr int kXWarps = 4;
+    static constexpr int kXBlocks = 3;
     struct Prim { double v[NV]; };
     struct Side { double v[NV]; };
 

@@ -165,17 +165,17 @@ __device__ __forceinline__ bool update_cell(const R* U, const R* Fp, const R* Fm
 // ---------------------------------------------------------------------------
 // x-sweep
 // ---------------------------------------------------------------------------
-// One CTA of XS_ROWS warps handles a 28-column tile over XS_ROWS * rpw rows:
-// warp w takes rows  row_block*XS_ROWS*rpw + w + k*XS_ROWS  (k < rpw) and loads
+// One CTA of WARPS warps handles a 28-column tile over WARPS * rpw rows:
+// warp w takes rows  row_block*WARPS*rpw + w + k*WARPS  (k < rpw) and loads
 // the next row's cells before computing the current one, so the load latency
 // overlaps the arithmetic.
-template <class PH>
+template <class PH, int WARPS = XS_ROWS>
 __device__ __forceinline__ void x_tile(const DevGrid& in, const DevGrid& out, const StepParams& P, double dt,
                                        double ch, int tile_x, int row_block, int rpw) {
     using R = typename PH::Real;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int row0 = row_block * XS_ROWS * rpw;
-    const int row_end = min(in.ny, row0 + XS_ROWS * rpw);
+    const int row0 = row_block * WARPS * rpw;
+    const int row_end = min(in.ny, row0 + WARPS * rpw);
     int row = row0 + warp;
     if (row >= row_end) return;  // whole warp: no block-level synchronisation follows
     const int ng = in.ng, ib = ng, ie = ng + in.nx;
@@ -194,12 +194,12 @@ __device__ __forceinline__ void x_tile(const DevGrid& in, const DevGrid& out, co
     if (xin) load_cell(in, x, ng + row, Unext);
 
 #pragma unroll 1
-    for (; row < row_end; row += XS_ROWS) {
+    for (; row < row_end; row += WARPS) {
         const int y = ng + row;
         R U[NV], W[NV];
 #pragma unroll
         for (int k = 0; k < NV; ++k) U[k] = Unext[k];
-        if (xin && row + XS_ROWS < row_end) load_cell(in, x, y + XS_ROWS, Unext);  // prefetch
+        if (xin && row + WARPS < row_end) load_cell(in, x, y + WARPS, Unext);  // prefetch
         PH::prim(U, g, W);
 
         typename PH::Side L, Rt;
@@ -231,8 +231,11 @@ __device__ __forceinline__ void x_tile(const DevGrid& in, const DevGrid& out, co
     }
 }
 
+// CTA shape and register budget per policy: PH::kXWarps warps per CTA,
+// PH::kXBlocks CTAs per SM.
 template <class PH>
-__global__ void __launch_bounds__(32 * XS_ROWS) sweep_x_kernel(DevGrid in, DevGrid out, StepParams P, int rpw) {
+__global__ void __launch_bounds__(32 * PH::kXWarps, PH::kXBlocks)
+    sweep_x_kernel(DevGrid in, DevGrid out, StepParams P, int rpw) {
     using R = typename PH::Real;
     double dt, ch, damp;
     const bool first = (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0);
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(32 * XS_ROWS) sweep_x_kernel(DevGrid in, DevGr
     }
     if (first && P.clock) P.clock->maxbits[P.parity ^ 1] = 0ull;
     if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
-    x_tile<PH>(in, out, P, dt, ch, blockIdx.x, blockIdx.y, rpw);
+    x_tile<PH, PH::kXWarps>(in, out, P, dt, ch, blockIdx.x, blockIdx.y, rpw);
 }
 
 // ---------------------------------------------------------------------------
