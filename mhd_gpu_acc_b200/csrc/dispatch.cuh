@@ -49,8 +49,8 @@ cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
                 map, tmp, out, P, per);
         } else {
             const long long warps = (long long)y_strips(tmp) * bands;
-            const unsigned grid = (unsigned)((warps + YS_WARPS - 1) / YS_WARPS);
-            sweep_y_kernel<PH><<<grid, dim3(32, YS_WARPS), 0, st>>>(tmp, out, P, per);
+            const unsigned grid = (unsigned)((warps + PH::kYWarps - 1) / PH::kYWarps);
+            sweep_y_kernel<PH><<<grid, dim3(32, PH::kYWarps), 0, st>>>(tmp, out, P, per);
         }
     }
     return cudaGetLastError();

@@ -15,6 +15,7 @@ struct FastPolicy {
     using Real = float;
     static constexpr int NW = NV;
     static constexpr int NS = 2 * NV;
+    static constexpr int kYWarps = 4;   // y-sweep warps per CTA (side by side)
     static constexpr int kYBlocks = 3;  // y-sweep CTAs per SM the register budget is cut for
     // x-sweep: 4 warps per CTA, 4 CTAs per SM (128 registers).  Measured at
     // 4096^2 (HLLD, van Leer): 0.591 ms, against 0.612 ms for 8 x 2 and 0.651 ms

@@ -16,6 +16,7 @@ struct ExactPolicy {
     using Real = double;
     static constexpr int NW = NV;  // primitive values per cell
     static constexpr int NS = NV;  // values per reconstructed side state (U*)
+    static constexpr int kYWarps = 4;   // y-sweep warps per CTA (side by side)
     static constexpr int kYBlocks = 2;  // y-sweep CTAs per SM the register budget is cut for
     // x-sweep: 4 warps per CTA, 3 CTAs per SM (168 registers, a few spilled).
     // Measured at 4096^2 (HLLD, van Leer): 2.29 ms, against 2.65 ms for one CTA

@@ -349,7 +349,7 @@ __device__ __forceinline__ void clock_advance(const StepParams& P, double dt, do
 __host__ __device__ __forceinline__ int y_strips(const DevGrid& g) { return (g.ng + g.nx + 31) / 32; }
 
 template <class PH>
-__global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) sweep_y_kernel(DevGrid in, DevGrid out,
+__global__ void __launch_bounds__(32 * PH::kYWarps, PH::kYBlocks) sweep_y_kernel(DevGrid in, DevGrid out,
                                                                             StepParams P, int per) {
     using R = typename PH::Real;
     double dt, ch, damp;
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) sweep_y_kernel(De
     }
     if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
     const int strips = y_strips(in);
-    const int w = blockIdx.x * YS_WARPS + threadIdx.y;
+    const int w = blockIdx.x * PH::kYWarps + threadIdx.y;
     const int r0 = (w / strips) * per;
     double vmax = 0.0;
     unsigned reverts = 0;
