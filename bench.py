@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4096, help="grid side")
-    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -328,40 +328,59 @@ def run_ours(a, world, rank, local):
                 "traffic": traffic, "kernel": dom, "kernel_ms": dom_ms, "algorithmic_bytes": alg,
                 "peak_kind": kind, "sweep_ms": [mx, my]}
 
-    # e2e through the C ABI with pinned FP64 host buffers
+    # e2e through the C ABI with pinned FP64 host buffers: every step uploads a
+    # state, advances it one FP32-bulk step and downloads the result.  Steps are
+    # independent, so two workspaces on two streams take turns: step k's
+    # download overlaps step k+1's upload (the two copy directions run at once).
     e2e = None
     if rank == 0 or True:
-        U = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
-        T = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
-        ws = m.GpuWorkspace()
-        m.init_gpu_workspace(ws, U)
-        m.set_gpu_physics_gamma(ws, cfg.gamma)
-        ws.set_limiter(limiter)
-        ws.set_sweep_shape(a.xrpw, a.yband, a.ystage)
-        ws.set_stream(stream.cuda_stream)
+        lanes = []
         hin = torch.from_numpy(U0).pin_memory()
-        hout = torch.empty_like(hin).pin_memory()
-        a_in, a_out = hin.numpy(), hout.numpy()
-        for _ in range(2):  # warm-up
+        a_in = hin.numpy()
+        for _ in range(2):
+            U = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
+            T = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
+            ws = m.GpuWorkspace()
+            m.init_gpu_workspace(ws, U)
+            m.set_gpu_physics_gamma(ws, cfg.gamma)
+            ws.set_limiter(limiter)
+            ws.set_sweep_shape(a.xrpw, a.yband, a.ystage)
+            s = torch.cuda.Stream()
+            ws.set_stream(s.cuda_stream)
+            hout = torch.empty_like(hin).pin_memory()
+            lanes.append((U, T, ws, s, hout.numpy(), hout))
+
+        def e2e_step(k):
+            U, T, ws, _, a_out, _ = lanes[k % 2]
             ws.upload(U, a_in)
             ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
             ws.download(U, a_out)
-        ws.synchronize()
+
+        for k in range(4):  # warm-up
+            e2e_step(k)
+        torch.cuda.synchronize()
         barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(a.e2e_steps):
-            ws.upload(U, a_in)
-            ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
-            ws.download(U, a_out)
+        for _, _, _, s, _, _ in lanes:
+            s.wait_event(e0)
+        for k in range(a.e2e_steps):
+            e2e_step(k)
+        for _, _, _, s, _, _ in lanes:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            stream.wait_event(ev)
         e1.record(stream)
         torch.cuda.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1), world)
-        ws.destroy()
+        for _, _, ws, _, _, _ in lanes:
+            ws.destroy()
         nbytes = U0.nbytes
         e2e = {"value": world * cells * a.e2e_steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": a.e2e_steps,
-               "what": "per step: H2D of the FP64 SoA state from pinned memory, one FP32-bulk step, D2H of the state"}
+               "what": "per step: H2D of the FP64 SoA state from pinned memory, one FP32-bulk step (mhd_run), "
+                       "D2H of the state; two workspaces on two streams alternate, so one step's download "
+                       "overlaps the next step's upload"}
 
     cpu = None
     if world == 1 and rank == 0 and not a.no_cpu_baseline:
