@@ -2,10 +2,11 @@
 //
 // Each instance (its own grid, gamma, CFL, c_r, boundary types, t_end and
 // device clock) is cut into the same work units the single-grid sweeps use:
-// x units of 28 columns x (XS_ROWS * rpw) rows, y units of 32 columns x
-// (YS_WARPS * seg) rows.  The units of all instances form one global list
-// (prefix offsets in `first`, split by phase: first[0..n] for x, first[n+1..2n+1]
-// for y).  A persistent launch per sweep phase -- `ctas` CTAs striding over the
+// x units of 28 columns x (BX_WARPS * rpw) rows; y units of YS_WARPS
+// consecutive (strip, band) items of an instance, strip-fastest (a strip is 32
+// columns, a band seg rows), as the single-grid y-sweep orders its warps.  The units of all instances
+// form one global list (prefix offsets in `first`, split by phase: first[0..n]
+// for x, first[n+1..2n+1] for y).  A persistent launch per sweep phase -- `ctas` CTAs striding over the
 // list -- advances every instance; the kernel boundary between the x and y
 // phases is the only synchronisation a step needs, and a CUDA graph of two
 // steps replays the loop.  Instance k's unit 0 performs the clock duties the
@@ -16,11 +17,15 @@
 
 namespace mhd {
 
+constexpr int BX_WARPS = 4;  // warps per batched x-sweep CTA
+
 struct BatchInst {
     DevGrid U, T;
     StepParams P;  // physics, boundary types, t_end and clock of this instance
     int x_tiles, x_rblocks;
-    int y_strips, y_groups;
+    int y_strips, y_bands;   // 32-column strips; bands of seg rows
+    int y_units;             // ceil(strips * bands / YS_WARPS)
+    int pad_;
 };
 
 // largest k in [0, n) with first[k] <= u (first is non-decreasing, first[0] = 0)
@@ -35,7 +40,7 @@ __device__ __forceinline__ int find_instance(const int* first, int n, int u) {
 }
 
 template <class PH>
-__global__ void __launch_bounds__(32 * XS_ROWS) batch_x_kernel(const BatchInst* __restrict__ inst,
+__global__ void __launch_bounds__(32 * BX_WARPS, PH::kXBlocks) batch_x_kernel(const BatchInst* __restrict__ inst,
                                                               const int* __restrict__ first, int n, int parity,
                                                               int rpw) {
     const int total = __ldg(first + n);
@@ -51,12 +56,12 @@ __global__ void __launch_bounds__(32 * XS_ROWS) batch_x_kernel(const BatchInst* 
         }
         if (local == 0 && threadIdx.x == 0) P.clock->maxbits[parity ^ 1] = 0ull;
         const int tiles = inst[k].x_tiles;
-        x_tile<PH>(inst[k].U, inst[k].T, P, dt, ch, local % tiles, local / tiles, rpw);
+        x_tile<PH, BX_WARPS>(inst[k].U, inst[k].T, P, dt, ch, local % tiles, local / tiles, rpw);
     }
 }
 
 template <class PH>
-__global__ void __launch_bounds__(32 * YS_WARPS) batch_y_kernel(const BatchInst* __restrict__ inst,
+__global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) batch_y_kernel(const BatchInst* __restrict__ inst,
                                                                const int* __restrict__ first, int n, int parity,
                                                                int seg) {
     const int total = __ldg(first + n);
@@ -73,11 +78,12 @@ __global__ void __launch_bounds__(32 * YS_WARPS) batch_y_kernel(const BatchInst*
         }
         const int strips = inst[k].y_strips;
         const DevGrid& T = inst[k].T;
-        const int r0 = ((local / strips) * YS_WARPS + threadIdx.y) * seg;
+        const int item = local * YS_WARPS + threadIdx.y;
+        const int strip = item % strips, r0 = (item / strips) * seg;
         double vmax = 0.0;
         unsigned reverts = 0;
-        y_segment<PH>(T, inst[k].U, P, dt, ch, damp, local % strips, T.ng + r0, min(seg, T.ny - r0), vmax,
-                      reverts);
+        if (item < strips * inst[k].y_bands)
+            y_segment<PH>(T, inst[k].U, P, dt, ch, damp, strip, T.ng + r0, min(seg, T.ny - r0), vmax, reverts);
         y_fold(P, vmax, reverts);
         if (local == 0 && lead) clock_advance(P, dt, ch);
     }
@@ -90,7 +96,7 @@ struct BatchLaunch {
     cudaStream_t st;
     template <class PH>
     cudaError_t run() const {
-        if (which == 1) batch_x_kernel<PH><<<ctas, 32 * XS_ROWS, 0, st>>>(inst, first, n, parity, xrpw);
+        if (which == 1) batch_x_kernel<PH><<<ctas, 32 * BX_WARPS, 0, st>>>(inst, first, n, parity, xrpw);
         else batch_y_kernel<PH><<<ctas, dim3(32, YS_WARPS), 0, st>>>(inst, first + n + 1, n, parity, yseg);
         return cudaGetLastError();
     }

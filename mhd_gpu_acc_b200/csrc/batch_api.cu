@@ -80,13 +80,14 @@ int build_worklist(mhd_batch* b) {
     for (int i = 0; i < b->n; ++i) {
         mhd::BatchInst& I = b->host_inst[i];
         I.x_tiles = (b->desc[i].nx + mhd::XS_TX - 1) / mhd::XS_TX;
-        const int rows = mhd::XS_ROWS * b->tune.xrpw;
+        const int rows = mhd::BX_WARPS * b->tune.xrpw;
         I.x_rblocks = (b->desc[i].ny + rows - 1) / rows;
         I.y_strips = (b->desc[i].nx + b->desc[i].ng + 31) / 32;  // strips holding interior columns
-        const int nseg = (b->desc[i].ny + b->tune.yseg - 1) / b->tune.yseg;
-        I.y_groups = (nseg + mhd::YS_WARPS - 1) / mhd::YS_WARPS;
+        I.y_bands = (b->desc[i].ny + b->tune.yseg - 1) / b->tune.yseg;
+        I.y_units = (I.y_strips * I.y_bands + mhd::YS_WARPS - 1) / mhd::YS_WARPS;
+        I.pad_ = 0;
         b->first[i + 1] = b->first[i] + I.x_tiles * I.x_rblocks;
-        b->first[b->n + 1 + i + 1] = b->first[b->n + 1 + i] + I.y_strips * I.y_groups;
+        b->first[b->n + 1 + i + 1] = b->first[b->n + 1 + i] + I.y_units;
     }
     BCK(cudaMemcpyAsync(b->d_inst, b->host_inst.data(), sizeof(mhd::BatchInst) * b->n, cudaMemcpyHostToDevice,
                         b->stream));
@@ -116,7 +117,7 @@ int start_clocks(mhd_batch* b) {
 }
 
 void default_ctas(mhd_batch* b) {
-    if (b->tune.ctas_x <= 0) b->tune.ctas_x = 2 * b->nsm;
+    if (b->tune.ctas_x <= 0) b->tune.ctas_x = 3 * b->nsm;
     if (b->tune.ctas_y <= 0) b->tune.ctas_y = 3 * b->nsm;
 }
 
@@ -330,7 +331,7 @@ int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best_out) {
     BCK(cudaEventCreate(&e1));
     mhd_batch_tuning best = b->tune;
     const int xr[] = {2, 4, 8, 16};
-    const int xc[] = {1, 2};
+    const int xc[] = {2, 3, 4};
     const int ys[] = {16, 32, 64, 128};
     const int yc[] = {2, 3, 4};
     auto time_phase = [&](int which, float* ms) -> int {
