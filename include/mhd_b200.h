@@ -276,8 +276,9 @@ int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best);
 /* ---- discrete adjoint (no reference counterpart) ----
  * Gradient of J(a) = 1/2 sum_interior (rho(t_N; a) - rho_target)^2 with respect
  * to the 16 perturbation amplitudes a of mhd_initialise_orszag_tang
- * (b0 = 1/sqrt(4 pi)), after nsteps steps of the split step with HLL and the
- * given limiter on periodic [0,1]^2 (nx x ny, ng = 2).  The reverse pass
+ * (b0 = 1/sqrt(4 pi)), after nsteps steps of the split step with HLL (or HLLD,
+ * mhd_adjoint_set_solver) and the given limiter on periodic [0,1]^2 (nx x ny,
+ * ng = 2).  The reverse pass
  * differentiates the time step and c_h through the CFL argmax cell, the psi
  * damping and every branch the forward took, recomputing the trajectory from
  * checkpoints kept every `checkpoint_every` steps (0: about sqrt(nsteps)).
@@ -286,6 +287,10 @@ typedef struct mhd_adjoint mhd_adjoint;
 int mhd_adjoint_create(int nx, int ny, int dtype, int limiter, double gamma, double cfl, double cr, int nsteps,
                        int checkpoint_every, mhd_adjoint** out);
 int mhd_adjoint_destroy(mhd_adjoint* a);
+/* Riemann solver of forward and adjoint: MHD_HLL (default) or MHD_HLLD (its
+ * star and double-star regions, its fallbacks to HLL and the GLM psi / Bn
+ * overwrite are differentiated). */
+int mhd_adjoint_set_solver(mhd_adjoint* a, int solver);
 /* rho_target: ny x nx interior densities, row-major (j * nx + i). */
 int mhd_adjoint_set_target(mhd_adjoint* a, const double* rho_target);
 /* Forward solve only: J (needs a target; else 0) and optionally the final

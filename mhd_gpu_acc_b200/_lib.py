@@ -127,6 +127,7 @@ PROTOTYPES = {
     "mhd_batch_tune": (_I, [_P, _I, C.POINTER(mhd_batch_tuning)]),
     "mhd_adjoint_create": (_I, [_I, _I, _I, _I, _D, _D, _D, _I, _I, C.POINTER(_P)]),
     "mhd_adjoint_destroy": (_I, [_P]),
+    "mhd_adjoint_set_solver": (_I, [_P, _I]),
     "mhd_adjoint_set_target": (_I, [_P, _P]),
     "mhd_adjoint_forward": (_I, [_P, _P, _pd, _P]),
     "mhd_adjoint_gradient": (_I, [_P, _P, _pd, _P]),

@@ -8,7 +8,7 @@ import ctypes as C
 import numpy as np
 
 from ._lib import check, load
-from .solver import F64, Limiter
+from .solver import F64, Limiter, RiemannSolver
 
 
 def amplitudes(seed: int, sigma: float = 0.01) -> np.ndarray:
@@ -18,11 +18,14 @@ def amplitudes(seed: int, sigma: float = 0.01) -> np.ndarray:
 
 class OTAdjoint:
     def __init__(self, n: int = 512, nsteps: int = 400, dtype: int = F64, limiter: int = Limiter.VANLEER,
-                 gamma: float = 5.0 / 3.0, cfl: float = 0.4, cr: float = 0.18, checkpoint_every: int = 0):
+                 gamma: float = 5.0 / 3.0, cfl: float = 0.4, cr: float = 0.18, checkpoint_every: int = 0,
+                 solver: int = RiemannSolver.HLL):
         self.n, self.nsteps = n, nsteps
         self.ptr = C.c_void_p()
         check(load().mhd_adjoint_create(n, n, int(dtype), int(limiter), gamma, cfl, cr, nsteps, checkpoint_every,
                                         C.byref(self.ptr)), "mhd_adjoint_create")
+        if int(solver) != int(RiemannSolver.HLL):
+            check(load().mhd_adjoint_set_solver(self.ptr, int(solver)), "mhd_adjoint_set_solver")
 
     def set_target(self, rho: np.ndarray) -> None:
         r = np.ascontiguousarray(rho, dtype=np.float64)

@@ -1,6 +1,6 @@
-// adjoint.cu -- discrete adjoint of the split GLM-MHD step (HLL, van Leer or
-// minmod, periodic boundaries) and the Orszag-Tang gradient problem of the C ABI
-// (mhd_adjoint_*).
+// adjoint.cu -- discrete adjoint of the split GLM-MHD step (HLL or HLLD, van
+// Leer or minmod, periodic boundaries) and the Orszag-Tang gradient problem of
+// the C ABI (mhd_adjoint_*).
 //
 // Forward step n (the same kernels as mhd_advance, explicit dt_n and c_h,n):
 //   m_n = max(c_h,n-1, max_cells s(U^n)),  c_h,n = m_n,  dt_n = cfl dmin / m_n,
@@ -56,7 +56,7 @@ __device__ __forceinline__ void st(const DevGrid& g, int dir, int line, int p, R
 
 // lamIn = (sweep)^T lamOut along DIR for every interior line; lanes along the
 // sweep direction.  Writes lamIn at positions [ng-2, ng+n+2) of each line.
-template <typename R, int DIR, int LIM>
+template <typename R, int DIR, int LIM, int SOLVER>
 __global__ void __launch_bounds__(256) adj_sweep_kernel(DevGrid U, DevGrid lamOut, DevGrid lamIn, R g, R dtd, R ch,
                                                         double* acc) {
     const int lane = threadIdx.x & 31;
@@ -101,11 +101,11 @@ __global__ void __launch_bounds__(256) adj_sweep_kernel(DevGrid U, DevGrid lamOu
         zero(lLn);
         R lch = R(0), ldtd = R(0);
         if (do_face) {
-            hll(Rs, Ln, ch, g, F);
+            face<SOLVER>(Rs, Ln, ch, g, F);
 #pragma unroll
             for (int k = 0; k < NV; ++k) lF[k] = dtd * (lTn[k] - lT[k]);
             R lch_f = R(0);
-            hll_adj(Rs, Ln, ch, g, lF, lR, lLn, lch_f);
+            face_adj<SOLVER>(Rs, Ln, ch, g, lF, lR, lLn, lch_f);
             if (own) lch += lch_f;
         }
         R Fm[NV], lL[NV];
@@ -283,20 +283,27 @@ unsigned blocks_for(long long n) {
     return (unsigned)(b < 1 ? 1 : b);
 }
 
+template <typename R, int SOLVER>
+void launch_adj_sweep(int dir, int lim, unsigned blocks, const DevGrid& U, const DevGrid& lout, const DevGrid& lin,
+                      double g, double dtd, double ch, double* acc, cudaStream_t st) {
+    if (dir == 0 && lim == VANLEER)
+        adj_sweep_kernel<R, 0, VANLEER, SOLVER><<<blocks, 256, 0, st>>>(U, lout, lin, (R)g, (R)dtd, (R)ch, acc);
+    else if (dir == 0)
+        adj_sweep_kernel<R, 0, MINMOD, SOLVER><<<blocks, 256, 0, st>>>(U, lout, lin, (R)g, (R)dtd, (R)ch, acc);
+    else if (lim == VANLEER)
+        adj_sweep_kernel<R, 1, VANLEER, SOLVER><<<blocks, 256, 0, st>>>(U, lout, lin, (R)g, (R)dtd, (R)ch, acc);
+    else
+        adj_sweep_kernel<R, 1, MINMOD, SOLVER><<<blocks, 256, 0, st>>>(U, lout, lin, (R)g, (R)dtd, (R)ch, acc);
+}
+
 template <typename R>
-cudaError_t run_adj_sweep(int dir, int lim, const DevGrid& U, const DevGrid& lout, const DevGrid& lin, double g,
-                          double dtd, double ch, double* acc, cudaStream_t st) {
+cudaError_t run_adj_sweep(int dir, int lim, int solver, const DevGrid& U, const DevGrid& lout, const DevGrid& lin,
+                          double g, double dtd, double ch, double* acc, cudaStream_t st) {
     const int nline = dir == 0 ? U.ny : U.nx, nalong = dir == 0 ? U.nx : U.ny;
     const long long warps = (long long)nline * ((nalong + 4 + AT - 1) / AT);
     const unsigned blocks = (unsigned)((warps * 32 + 255) / 256);
-    if (dir == 0 && lim == VANLEER)
-        adj_sweep_kernel<R, 0, VANLEER><<<blocks, 256, 0, st>>>(U, lout, lin, (R)g, (R)dtd, (R)ch, acc);
-    else if (dir == 0)
-        adj_sweep_kernel<R, 0, MINMOD><<<blocks, 256, 0, st>>>(U, lout, lin, (R)g, (R)dtd, (R)ch, acc);
-    else if (lim == VANLEER)
-        adj_sweep_kernel<R, 1, VANLEER><<<blocks, 256, 0, st>>>(U, lout, lin, (R)g, (R)dtd, (R)ch, acc);
-    else
-        adj_sweep_kernel<R, 1, MINMOD><<<blocks, 256, 0, st>>>(U, lout, lin, (R)g, (R)dtd, (R)ch, acc);
+    if (solver == HLLD) launch_adj_sweep<R, HLLD>(dir, lim, blocks, U, lout, lin, g, dtd, ch, acc, st);
+    else launch_adj_sweep<R, HLL>(dir, lim, blocks, U, lout, lin, g, dtd, ch, acc, st);
     return cudaGetLastError();
 }
 
@@ -307,7 +314,7 @@ cudaError_t run_adj_sweep(int dir, int lim, const DevGrid& U, const DevGrid& lou
 // host orchestration
 // ---------------------------------------------------------------------------
 struct mhd_adjoint {
-    int nx = 0, ny = 0, dtype = MHD_F64, limiter = MHD_LIMITER_VANLEER, nsteps = 0, every = 1;
+    int nx = 0, ny = 0, dtype = MHD_F64, limiter = MHD_LIMITER_VANLEER, solver = MHD_HLL, nsteps = 0, every = 1;
     double gamma = 5.0 / 3.0, cfl = 0.4, cr = 0.18, b0 = 0.0;
     std::vector<mhd_grid> ckpt, seg;
     mhd_grid T{}, lamA{}, lamB{}, lamT{}, lamV{};
@@ -358,7 +365,7 @@ const int kPeriodic[4] = {MHD_BC_PERIODIC, MHD_BC_PERIODIC, MHD_BC_PERIODIC, MHD
 // one forward step Uin -> Uout through the library's step with explicit dt / ch
 int fwd_step(mhd_adjoint* a, const mhd_grid& Uin, mhd_grid& Uout, double dt, double ch) {
     ARC(mhd_set_ch(a->ws, ch));
-    return mhd_advance(a->ws, &Uin, &a->T, &Uout, dt, MHD_HLL, kPeriodic);
+    return mhd_advance(a->ws, &Uin, &a->T, &Uout, dt, a->solver, kPeriodic);
 }
 
 // Forward solve from amp: checkpoints every `every` steps, per-step dt and ch.
@@ -376,7 +383,7 @@ int forward(mhd_adjoint* a, const double* amp, double* J, double* rho_final) {
         ARC(mhd_compute_dt(a->ws, &cur, a->cfl, &dt));
         ARC(mhd_get_ch(a->ws, &a->ch[n]));
         a->dt[n] = dt;
-        ARC(mhd_advance(a->ws, &cur, &a->T, &nxt, dt, MHD_HLL, kPeriodic));
+        ARC(mhd_advance(a->ws, &cur, &a->T, &nxt, dt, a->solver, kPeriodic));
         std::swap(cur, nxt);
     }
     // keep the final state in seg[0] for the objective
@@ -425,14 +432,14 @@ int reverse_step(mhd_adjoint* a, int n, const mhd_grid& Un, const mhd_grid& Un1,
     {
         mhd::StepParams P{};
         P.gamma = a->gamma; P.cr = a->cr; P.dx = dx; P.dy = dy; P.dmin = dx < dy ? dx : dy;
-        P.dt = dt; P.ch = ch; P.damp = f; P.solver = MHD_HLL; P.limiter = a->limiter;
+        P.dt = dt; P.ch = ch; P.damp = f; P.solver = a->solver; P.limiter = a->limiter;
         const cudaError_t e = f64(a) ? mhd::launch_step_f64(dg(Un), dg(a->T), dg(a->T), P, st, mhd::kDefaultYBand, 1)
                                      : mhd::launch_step_f32(dg(Un), dg(a->T), dg(a->T), P, st, mhd::kDefaultYBand, 1);
         ACK(e);
     }
     // (c) lambda_T = Y^T lambda_V
     ARC(zero_grid(a->lamT, st));
-    ACK(mhd::adj::run_adj_sweep<R>(1, a->limiter, dg(a->T), dg(a->lamV), dg(a->lamT), a->gamma, dt / dy, ch,
+    ACK(mhd::adj::run_adj_sweep<R>(1, a->limiter, a->solver, dg(a->T), dg(a->lamV), dg(a->lamT), a->gamma, dt / dy, ch,
                                    a->d_acc, st));
     double s_y[2];
     ACK(cudaMemcpy(s_y, a->d_acc, sizeof s_y, cudaMemcpyDeviceToHost));
@@ -443,7 +450,7 @@ int reverse_step(mhd_adjoint* a, int n, const mhd_grid& Un, const mhd_grid& Un1,
     ACK(cudaGetLastError());
     // (e) lambda_U = X^T lambda_T
     ARC(zero_grid(lam_out, st));
-    ACK(mhd::adj::run_adj_sweep<R>(0, a->limiter, dg(Un), dg(a->lamV), dg(lam_out), a->gamma, dt / dx, ch,
+    ACK(mhd::adj::run_adj_sweep<R>(0, a->limiter, a->solver, dg(Un), dg(a->lamV), dg(lam_out), a->gamma, dt / dx, ch,
                                    a->d_acc, st));
     double s_x[2];
     ACK(cudaMemcpy(s_x, a->d_acc, sizeof s_x, cudaMemcpyDeviceToHost));
@@ -543,6 +550,14 @@ int mhd_adjoint_create(int nx, int ny, int dtype, int limiter, double gamma, dou
         return rc;
     }
     *out = a;
+    return MHD_OK;
+}
+
+int mhd_adjoint_set_solver(mhd_adjoint* a, int solver) {
+    if (!a) return aerr(MHD_ERR_STATE, "mhd_adjoint_set_solver: null adjoint");
+    if (solver != MHD_HLL && solver != MHD_HLLD)
+        return aerr(MHD_ERR_ARG, "mhd_adjoint_set_solver: the adjoint differentiates HLL or HLLD");
+    a->solver = solver;
     return MHD_OK;
 }
 

@@ -142,6 +142,50 @@ int main() {
             if (b1 == br && b2 == br) report("speed", ad, fd);
         }
     }
+    // HLLD face (with the GLM overwrite and the HLL fallbacks): states spread so
+    // that every region is taken; a check counts only when both perturbed
+    // evaluations stay in the region of the base point.
+    int hits[7] = {0};
+    for (int trial = 0; trial < 6000; ++trial) {
+        double WL[NV], WR[NV], UL[NV], UR[NV], dL[NV], dR[NV], w[NV];
+        rand_prim(WL);
+        rand_prim(WR);
+        WL[PU] = uni(-2.5, 2.5);
+        WR[PU] = WL[PU] + uni(-1.5, 1.5);
+        WL[BX] = uni(-1.5, 1.5);
+        WR[BX] = WL[BX] + uni(-0.2, 0.2);
+        WL[PP] = uni(0.05, 2.0);
+        p2c(WL, g, UL);
+        p2c(WR, g, UR);
+        for (int k = 0; k < NV; ++k) { dL[k] = uni(-1, 1); dR[k] = uni(-1, 1); w[k] = uni(-1, 1); }
+        const double ch = uni(0.2, 3.0), dch = uni(-1, 1);
+        HlldState<double> s0, sp, sm;
+        double Lp[NV], Lm[NV], Rp[NV], Rm[NV];
+        for (int k = 0; k < NV; ++k) {
+            Lp[k] = UL[k] + h * dL[k]; Lm[k] = UL[k] - h * dL[k];
+            Rp[k] = UR[k] + h * dR[k]; Rm[k] = UR[k] - h * dR[k];
+        }
+        hlld_state(UL, UR, ch, g, s0);
+        hlld_state(Lp, Rp, ch + h * dch, g, sp);
+        hlld_state(Lm, Rm, ch - h * dch, g, sm);
+        if (sp.region != s0.region || sm.region != s0.region) continue;
+        hits[s0.region + 1]++;
+        double lL[NV] = {0}, lR[NV] = {0}, lch = 0, a[NV], b[NV];
+        face_adj<HLLD>(UL, UR, ch, g, w, lL, lR, lch);
+        face<HLLD>(Lp, Rp, ch + h * dch, g, a);
+        face<HLLD>(Lm, Rm, ch - h * dch, g, b);
+        double fd = 0, ad = lch * dch;
+        for (int k = 0; k < NV; ++k) { fd += w[k] * (a[k] - b[k]) / (2 * h); ad += lL[k] * dL[k] + lR[k] * dR[k]; }
+        static const char* names[7] = {"hlld_hll", "hlld_FL", "hlld_FR", "hlld_L*", "hlld_L**", "hlld_R*", "hlld_R**"};
+        report(names[s0.region + 1], ad, fd);
+    }
+    std::printf("HLLD regions checked (HLL, FL, FR, L*, L**, R*, R**): %d %d %d %d %d %d %d\n", hits[0], hits[1],
+                hits[2], hits[3], hits[4], hits[5], hits[6]);
+    for (int r = 1; r < 7; ++r)
+        if (hits[r] < 20) {
+            std::printf("HLLD region %d checked only %d times\n", r - 1, hits[r]);
+            return 1;
+        }
     std::printf("worst relative error %.3e\n", worst);
     return worst < 1e-5 ? 0 : 1;
 }

@@ -2,7 +2,7 @@
 FP64 central finite differences, FP32 against FP64, checkpoint independence,
 and a torch.autograd.Function wrapper checked with torch.autograd.gradcheck.
 
-The gradient problem: Orszag-Tang on periodic [0,1]^2, HLL + van Leer, 16
+The gradient problem: Orszag-Tang on periodic [0,1]^2, HLL (or HLLD) + van Leer, 16
 Fourier amplitudes a ~ N(0, 0.01^2) (seed s) perturbing v and B, target density
 from a second amplitude set (seed s + 1), J = 1/2 sum (rho - rho_target)^2.
 """
@@ -29,8 +29,8 @@ def test_local_adjoints_against_finite_differences(tmp_path):
     assert r.returncode == 0, r.stdout
 
 
-def _problem(n, steps, dtype=F64, seed=0, every=0):
-    adj = OTAdjoint(n=n, nsteps=steps, dtype=dtype, checkpoint_every=every)
+def _problem(n, steps, dtype=F64, seed=0, every=0, solver=0):
+    adj = OTAdjoint(n=n, nsteps=steps, dtype=dtype, checkpoint_every=every, solver=solver)
     _, target = adj.forward(amplitudes(seed + 1), want_rho=True)
     adj.set_target(target)
     return adj, amplitudes(seed)
@@ -52,6 +52,21 @@ def test_gradient_matches_central_differences_small():
     fd = _fd(adj, a)
     assert J > 0
     assert np.linalg.norm(g - fd) / np.linalg.norm(fd) <= FD_RTOL, (g, fd)
+
+
+@pytest.mark.gpu
+def test_hlld_gradient_matches_central_differences():
+    """The HLLD adjoint (star / double-star regions, HLL fallbacks, GLM
+    overwrite) on the same problem: FP64 against central differences, FP32
+    against FP64."""
+    adj, a = _problem(64, 40, solver=2)
+    J, g = adj.gradient(a)
+    fd = _fd(adj, a)
+    assert J > 0
+    assert np.linalg.norm(g - fd) / np.linalg.norm(fd) <= FD_RTOL, (g, fd)
+    adj32, _ = _problem(64, 40, F32, solver=2)
+    _, g32 = adj32.gradient(a)
+    assert np.linalg.norm(g32 - g) / np.linalg.norm(g) <= 1e-2
 
 
 @pytest.mark.gpu
