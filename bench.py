@@ -52,9 +52,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="ot", choices=["ot", "batch", "adjoint"],
+    ap.add_argument("--workload", default="ot", choices=["ot", "batch", "adjoint", "precision"],
                     help="ot: Orszag-Tang n^2 (default line); batch: 256 uneven Orszag-Tang instances; "
-                         "adjoint: gradient of the Orszag-Tang objective")
+                         "adjoint: gradient of the Orszag-Tang objective; precision: FP32-bulk vs FP64 "
+                         "relative L1 / Linf per field of every configuration, run to t_end")
+    ap.add_argument("--precision-max-n", type=int, default=2048,
+                    help="largest Orszag-Tang side of the precision workload (512, 2048, 4096)")
     ap.add_argument("--seed", type=int, default=0, help="batch workload seed")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--xrpw", type=int, default=8, help="x-sweep rows per warp")
@@ -566,6 +569,75 @@ def run_adjoint(a, world, rank, local):
     return 0
 
 
+FIELDS = ["rho", "rhou", "rhov", "rhow", "Bx", "By", "Bz", "E", "psi"]
+
+
+def run_precision(a, world, rank, local):
+    """Every configuration run with the FP64 step and with the FP32-bulk step
+    (device-resident loop); relative L1 (sum|a-b| / sum|b|) and Linf
+    (max|a-b| / max|b|) of the interior, per conserved field.  Orszag-Tang and
+    Brio-Wu run to t_end.  The Mach-10 shock-bubble runs 500 steps: with the
+    reference's scheme (no positivity guard on the update) its pressure turns
+    negative once the shock has crossed the dense bubble and the time step
+    collapses before t_end -- the reference's own CPU code stops at step 1069 of
+    the 512^2 case (t = 0.040), as does the FP64 step here, and at 2048^2 the
+    HLLC run stops at step 638.
+    Beside each FP32 error stands the FP64 step's own sensitivity: FP64 from
+    initial data perturbed by a relative 1e-12 (seeded), against FP64 -- where
+    that is large, the flow amplifies rounding-level differences and no
+    arithmetic that is not bit-identical to the FP64 step can agree closer."""
+    import numpy as np
+    import torch
+
+    import mhd_gpu_acc_b200 as m
+
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return 0
+    H, HC, VL, MM = m.RiemannSolver.HLLD, m.RiemannSolver.HLLC, m.Limiter.VANLEER, m.Limiter.MINMOD
+    cases = [(f"orszag_tang_{n}_hlld_vanleer", m.CaseId.OrszagTangUnit, n, n, H, VL, 0)
+             for n in (512, 2048, 4096) if n <= a.precision_max_n]
+    cases += [("shock_bubble_2048_hllc_500_steps", m.CaseId.ShockBubbleMHD, 2048, 2048, HC, MM, 500),
+              ("shock_bubble_2048_hlld_500_steps", m.CaseId.ShockBubbleMHD, 2048, 2048, H, MM, 500),
+              ("brio_wu_800x4_hlld_cfl0.8", m.CaseId.BrioWuCFL08, 800, 4, H, MM, 0)]
+    out = {}
+    for name, case, nx, ny, solver, lim, max_steps in cases:
+        cfg = m.get_n_case_config(case, 1)
+        U0 = m.initialise(case, nx, ny, 2, cfg.extent)
+        res = {}
+        P0 = U0 * (1.0 + 1e-12 * np.random.default_rng(1).standard_normal(U0.shape))
+        for key, dt, init in (("f64", m.F64, U0), ("f32", m.F32, U0), ("f64p", m.F64, P0)):
+            U = m.Grid2DGPU(nx, ny, 2, *cfg.extent, dt)
+            T = m.Grid2DGPU(nx, ny, 2, *cfg.extent, dt)
+            ws = m.GpuWorkspace()
+            m.init_gpu_workspace(ws, U)
+            m.set_gpu_physics_gamma(ws, cfg.gamma)
+            m.set_gpu_physics_ch(ws, 0.0)
+            ws.set_limiter(lim)
+            U.upload(init)
+            info = ws.run(U, T, cfg.cfl, cfg.t_end, max_steps, solver, cfg.bc)
+            res[key] = (U.download()[:, 2:-2, 2:-2], info.steps, info.t)
+            ws.destroy()
+            del U, T
+        a64, s64, t64 = res["f64"]
+        b_ = np.abs(a64).reshape(9, -1)
+
+        def errs(other):
+            d = np.abs(other - a64).reshape(9, -1)
+            l1 = [float(d[k].sum() / b_[k].sum()) if b_[k].sum() > 0 else float(d[k].sum()) for k in range(9)]
+            li = [float(d[k].max() / b_[k].max()) if b_[k].max() > 0 else float(d[k].max()) for k in range(9)]
+            return dict(zip(FIELDS, l1)), dict(zip(FIELDS, li))
+
+        l1, li = errs(res["f32"][0])
+        pl1, _ = errs(res["f64p"][0])
+        out[name] = {"steps_fp64": s64, "steps_fp32": res["f32"][1], "t": t64,
+                     "rel_l1": l1, "rel_linf": li, "fp64_perturbed_1e-12_rel_l1": pl1}
+    print(json.dumps({"metric": "FP32-bulk vs FP64 relative error per field of each configuration",
+                      "unit": "relative", "n_gpus": 1, "dtype": "f32 vs f64", "data": "synthetic (library initial data)",
+                      "config": {"workload": "precision", "cases": list(out)}, "cases": out}))
+    return 0
+
+
 def main():
     a = parse()
     world, rank, local = dist_setup()
@@ -575,6 +647,8 @@ def main():
         return run_batch(a, world, rank, local)
     if a.workload == "adjoint":
         return run_adjoint(a, world, rank, local)
+    if a.workload == "precision":
+        return run_precision(a, world, rank, local)
     return run_ours(a, world, rank, local)
 
 
