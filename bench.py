@@ -331,14 +331,15 @@ def run_ours(a, world, rank, local):
                 "traffic": traffic, "kernel": dom, "kernel_ms": dom_ms, "algorithmic_bytes": alg,
                 "peak_kind": kind, "sweep_ms": [mx, my]}
 
-    # e2e through the C ABI with pinned FP64 host buffers: every step uploads a
-    # state, advances it one FP32-bulk step and downloads the result.  Steps are
-    # independent, so two workspaces on two streams take turns: step k's
-    # download overlaps step k+1's upload (the two copy directions run at once).
+    # e2e through the C ABI with pinned FP32 host buffers (the FP32-bulk step's
+    # own state format): every step uploads a state, advances it one FP32-bulk
+    # step and downloads the result.  Steps are independent, so two workspaces
+    # on two streams take turns: step k's download overlaps step k+1's upload
+    # (the two copy directions run at once).
     e2e = None
     if rank == 0 or True:
         lanes = []
-        hin = torch.from_numpy(U0).pin_memory()
+        hin = torch.from_numpy(U0.astype(np.float32)).pin_memory()
         a_in = hin.numpy()
         for _ in range(2):
             U = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
@@ -355,9 +356,9 @@ def run_ours(a, world, rank, local):
 
         def e2e_step(k):
             U, T, ws, _, a_out, _ = lanes[k % 2]
-            ws.upload(U, a_in)
+            ws.upload_f32(U, a_in)
             ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
-            ws.download(U, a_out)
+            ws.download_f32(U, a_out)
 
         for k in range(4):  # warm-up
             e2e_step(k)
@@ -378,12 +379,12 @@ def run_ours(a, world, rank, local):
         ms = max_over_ranks(e0.elapsed_time(e1), world)
         for _, _, ws, _, _, _ in lanes:
             ws.destroy()
-        nbytes = U0.nbytes
+        nbytes = int(hin.numel() * hin.element_size())
         e2e = {"value": world * cells * a.e2e_steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": a.e2e_steps,
-               "what": "per step: H2D of the FP64 SoA state from pinned memory, one FP32-bulk step (mhd_run), "
-                       "D2H of the state; two workspaces on two streams alternate, so one step's download "
-                       "overlaps the next step's upload"}
+               "what": "per step: H2D of the FP32 SoA state (ghosts included) from pinned memory "
+                       "(mhd_upload_f32), one FP32-bulk step (mhd_run), D2H of the state (mhd_download_f32); two "
+                       "workspaces on two streams alternate, so one step's download overlaps the next step's upload"}
 
     cpu = None
     if world == 1 and rank == 0 and not a.no_cpu_baseline:

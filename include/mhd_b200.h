@@ -196,6 +196,11 @@ int mhd_profile_sweeps(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, 
  * buffer (pinned host memory gives full bandwidth).  Same layout as mhd_grid_upload. */
 int mhd_upload(mhd_workspace* ws, const mhd_grid* g, const double* host);
 int mhd_download(mhd_workspace* ws, const mhd_grid* g, double* host);
+/* The same for an FP32 grid with FP32 host arrays (dense (9, ny+2ng, nx+2ng)):
+ * half the bytes of the FP64 host format and no device-side conversion.  No
+ * reference counterpart. */
+int mhd_upload_f32(mhd_workspace* ws, const mhd_grid* g, const float* host);
+int mhd_download_f32(mhd_workspace* ws, const mhd_grid* g, float* host);
 int mhd_synchronize(mhd_workspace* ws);
 
 /* FP64 diagnostics of a state: out[0] = sum rho dA, out[1] = sum E dA,

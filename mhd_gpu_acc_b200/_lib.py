@@ -108,6 +108,8 @@ PROTOTYPES = {
     "mhd_profile_sweeps": (_I, [_P, _pg, _pg, _D, _D, _I, _pi, _I, C.POINTER(C.c_float)]),
     "mhd_upload": (_I, [_P, _pg, _P]),
     "mhd_download": (_I, [_P, _pg, _P]),
+    "mhd_upload_f32": (_I, [_P, _pg, _P]),
+    "mhd_download_f32": (_I, [_P, _pg, _P]),
     "mhd_synchronize": (_I, [_P]),
     "mhd_diagnostics": (_I, [_P, _pg, _pd]),
     "mhd_case_config": (_I, [_I, _I, _pd]),

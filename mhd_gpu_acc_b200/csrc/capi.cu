@@ -713,6 +713,30 @@ int mhd_upload(mhd_workspace* ws, const mhd_grid* g, const double* host) {
     return upload_impl(g, host, ws->d_stage, ws->stream);
 }
 
+// FP32 host arrays for FP32 grids: one pitched copy per field, no staging.
+static int copy_f32(mhd_workspace* ws, const mhd_grid* g, float* host, bool up, const char* what) {
+    int rc = check_ws_grid(ws, g, what);
+    if (rc) return rc;
+    if (!host) return fail(MHD_ERR_ARG, "%s: null host pointer", what);
+    if (g->dtype != MHD_F32) return fail(MHD_ERR_ARG, "%s: the grid is not FP32", what);
+    const long long tnx = g->nx + 2LL * g->ng, tny = g->ny + 2LL * g->ng;
+    for (int f = 0; f < MHD_NV; ++f) {
+        float* d = static_cast<float*>(g->data) + f * g->plane;
+        float* h = host + f * tnx * tny;
+        if (up) CK(cudaMemcpy2DAsync(d, g->pitch * 4, h, tnx * 4, tnx * 4, tny, cudaMemcpyHostToDevice, ws->stream));
+        else CK(cudaMemcpy2DAsync(h, tnx * 4, d, g->pitch * 4, tnx * 4, tny, cudaMemcpyDeviceToHost, ws->stream));
+    }
+    return MHD_OK;
+}
+
+int mhd_upload_f32(mhd_workspace* ws, const mhd_grid* g, const float* host) {
+    return copy_f32(ws, g, const_cast<float*>(host), true, "mhd_upload_f32");
+}
+
+int mhd_download_f32(mhd_workspace* ws, const mhd_grid* g, float* host) {
+    return copy_f32(ws, g, host, false, "mhd_download_f32");
+}
+
 int mhd_download(mhd_workspace* ws, const mhd_grid* g, double* host) {
     int rc = check_ws_grid(ws, g, "mhd_download");
     if (rc) return rc;

@@ -255,6 +255,15 @@ class GpuWorkspace:
     def download(self, grid: Grid2DGPU, host: np.ndarray) -> None:
         check(load().mhd_download(self._req(), C.byref(grid.g), host.ctypes.data), "mhd_download")
 
+    def upload_f32(self, grid: Grid2DGPU, host: np.ndarray) -> None:
+        """FP32 host array (9, ny+2ng, nx+2ng) -> FP32 grid, asynchronous on the workspace stream."""
+        assert host.dtype == np.float32 and host.flags.c_contiguous and host.shape == grid.shape
+        check(load().mhd_upload_f32(self._req(), C.byref(grid.g), host.ctypes.data), "mhd_upload_f32")
+
+    def download_f32(self, grid: Grid2DGPU, host: np.ndarray) -> None:
+        assert host.dtype == np.float32 and host.flags.c_contiguous and host.shape == grid.shape
+        check(load().mhd_download_f32(self._req(), C.byref(grid.g), host.ctypes.data), "mhd_download_f32")
+
     def synchronize(self) -> None:
         check(load().mhd_synchronize(self._req()), "mhd_synchronize")
 

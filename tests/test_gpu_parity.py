@@ -218,6 +218,33 @@ def test_aos_round_trip():
     np.testing.assert_array_equal(h.download_to_aos(), aos.astype(np.float32).astype(np.float64))
 
 
+def test_fp32_host_copies():
+    """FP32 host arrays in and out of an FP32 grid equal the FP64 host path's
+    rounding of the same data; an FP64 grid refuses them."""
+    rng = np.random.default_rng(4)
+    host = rng.standard_normal((9, 17, 21))
+    g = Grid2DGPU(17, 13, 2, 0.0, 1.0, 0.0, 1.0, F32)
+    ws = GpuWorkspace()
+    init_gpu_workspace(ws, g)
+    h32 = host.astype(np.float32)
+    ws.upload_f32(g, h32)
+    out = np.empty_like(h32)
+    ws.download_f32(g, out)
+    ws.synchronize()
+    np.testing.assert_array_equal(out, h32)
+    g.upload(host)
+    ws.download_f32(g, out)
+    ws.synchronize()
+    np.testing.assert_array_equal(out, h32)
+    g64 = Grid2DGPU(17, 13, 2, 0.0, 1.0, 0.0, 1.0, F64)
+    ws64 = GpuWorkspace()
+    init_gpu_workspace(ws64, g64)
+    with pytest.raises(MhdError):
+        ws64.upload_f32(g64, h32)
+    ws.destroy()
+    ws64.destroy()
+
+
 def test_reference_error_behaviour():
     a = Grid2DGPU(16, 16, 2, 0.0, 1.0, 0.0, 1.0, F64)
     b = Grid2DGPU(16, 8, 2, 0.0, 1.0, 0.0, 1.0, F64)
