@@ -163,11 +163,11 @@ MHD_HD_INLINE void hll(const double* UL, const double* UR, double ch, double g, 
 }
 
 template <int DIR>
-MHD_HD_INLINE void hllc(const double* UL, const double* UR, double ch, double g, double* F) {
+MHD_HD_INLINE bool hllc_star(const double* UL, const double* UR, double ch, double g, double* F) {
     double VL[NV], VR[NV];
     c2p(UL, g, VL);
     c2p(UR, g, VR);
-    if (!riemann_physical(VL) || !riemann_physical(VR)) { hll<DIR>(UL, UR, ch, g, F); return; }
+    if (!riemann_physical(VL) || !riemann_physical(VR)) return false;
     const double rhoL = VL[RHO], rhoR = VR[RHO];
     const double pL = VL[PP], pR = VR[PP];
     double unL, unR, utL, utR, uwL, uwR, BnL, BnR, BtL, BtR, BwL, BwR;
@@ -183,12 +183,12 @@ MHD_HD_INLINE void hllc(const double* UL, const double* UR, double ch, double g,
     if (SL >= 0.0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = FL[k];
-        return;
+        return true;
     }
     if (SR <= 0.0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = FR[k];
-        return;
+        return true;
     }
     const double BmagL2 = BnL * BnL + BtL * BtL + BwL * BwL;
     const double BmagR2 = BnR * BnR + BtR * BtR + BwR * BwR;
@@ -196,14 +196,11 @@ MHD_HD_INLINE void hllc(const double* UL, const double* UR, double ch, double g,
     const double ptR = pR + 0.5 * BmagR2;
     const double numerSM = (SR - unR) * rhoR * unR - (SL - unL) * rhoL * unL + ptL - ptR;
     const double denomSM = (SR - unR) * rhoR - (SL - unL) * rhoL;
-    if (fabs(denomSM) < 1.0e-14) { hll<DIR>(UL, UR, ch, g, F); return; }
+    if (fabs(denomSM) < 1.0e-14) return false;
     const double SM = numerSM / denomSM;
     const double rhoLs = rhoL * (SL - unL) / (SL - SM);
     const double rhoRs = rhoR * (SR - unR) / (SR - SM);
-    if (rhoLs <= 0.0 || rhoRs <= 0.0 || !isfinite(rhoLs) || !isfinite(rhoRs)) {
-        hll<DIR>(UL, UR, ch, g, F);
-        return;
-    }
+    if (rhoLs <= 0.0 || rhoRs <= 0.0 || !isfinite(rhoLs) || !isfinite(rhoRs)) return false;
     const double ptLs = ptL + rhoL * (SL - unL) * (SM - unL);
     const double ptRs = ptR + rhoR * (SR - unR) * (SM - unR);
     const double psiM = 0.5 * (VL[PSI] + VR[PSI]) - 0.5 * ch * (BnR - BnL);
@@ -223,14 +220,21 @@ MHD_HD_INLINE void hllc(const double* UL, const double* UR, double ch, double g,
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = FR[k] + SR * (Us[k] - UR[k]);
     }
+    return true;
+}
+
+// hllc as a whole (the star solver or, where it gives up, HLL).
+template <int DIR>
+MHD_HD_INLINE void hllc(const double* UL, const double* UR, double ch, double g, double* F) {
+    if (!hllc_star<DIR>(UL, UR, ch, g, F)) hll<DIR>(UL, UR, ch, g, F);
 }
 
 template <int DIR>
-MHD_HD_INLINE void hlld(const double* UL, const double* UR, double ch, double g, double* F) {
+MHD_HD_INLINE bool hlld_star(const double* UL, const double* UR, double ch, double g, double* F) {
     double VL[NV], VR[NV];
     c2p(UL, g, VL);
     c2p(UR, g, VR);
-    if (!riemann_physical(VL) || !riemann_physical(VR)) { hll<DIR>(UL, UR, ch, g, F); return; }
+    if (!riemann_physical(VL) || !riemann_physical(VR)) return false;
     const double rhoL = VL[RHO], rhoR = VR[RHO];
     const double pL = VL[PP], pR = VR[PP];
     double unL, unR, utL, utR, uwL, uwR, BnL, BnR, BtL, BtR, BwL, BwR;
@@ -241,7 +245,7 @@ MHD_HD_INLINE void hlld(const double* UL, const double* UR, double ch, double g,
     const double SL = fmin(unL - cfL, unR - cfR);
     const double SR = fmax(unL + cfL, unR + cfR);
     const double denom_RL = SR - SL;
-    if (fabs(denom_RL) < 1.0e-14) { hll<DIR>(UL, UR, ch, g, F); return; }
+    if (fabs(denom_RL) < 1.0e-14) return false;
     double FL[NV], FR[NV];
     // The outer-region early returns come last in the reference
     // (head/riemann.hpp:448-449) but only after fallbacks to HLL that produce
@@ -252,25 +256,22 @@ MHD_HD_INLINE void hlld(const double* UL, const double* UR, double ch, double g,
     const double ptR = pR + 0.5 * BmagR2;
     const double numerSM = (SR - unR) * rhoR * unR - (SL - unL) * rhoL * unL + ptL - ptR;
     const double denomSM = (SR - unR) * rhoR - (SL - unL) * rhoL;
-    if (fabs(denomSM) < 1.0e-14) { hll<DIR>(UL, UR, ch, g, F); return; }
+    if (fabs(denomSM) < 1.0e-14) return false;
     const double SM = numerSM / denomSM;
     const double rhoLs = rhoL * (SL - unL) / (SL - SM);
     const double rhoRs = rhoR * (SR - unR) / (SR - SM);
-    if (rhoLs <= 0.0 || rhoRs <= 0.0 || !isfinite(rhoLs) || !isfinite(rhoRs)) {
-        hll<DIR>(UL, UR, ch, g, F);
-        return;
-    }
+    if (rhoLs <= 0.0 || rhoRs <= 0.0 || !isfinite(rhoLs) || !isfinite(rhoRs)) return false;
     flux<DIR>(UL, ch, g, FL);
     flux<DIR>(UR, ch, g, FR);
     if (SL >= 0.0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = FL[k];
-        return;
+        return true;
     }
     if (SR <= 0.0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = FR[k];
-        return;
+        return true;
     }
     const double ptstar = ptL + rhoL * (SL - unL) * (SM - unL);
     const double sqrtRhoLs = sqrt(rhoLs);
@@ -296,7 +297,7 @@ MHD_HD_INLINE void hlld(const double* UL, const double* UR, double ch, double g,
         if (SLs >= 0.0) {
 #pragma unroll
             for (int k = 0; k < NV; ++k) F[k] = FL[k] + SL * (Us[k] - UL[k]);
-            return;
+            return true;
         }
         // L** needs the R* state as well (head/riemann.hpp:357-413)
         double utRs, uwRs, BtRs, BwRs;
@@ -348,7 +349,7 @@ MHD_HD_INLINE void hlld(const double* UL, const double* UR, double ch, double g,
         if (SRs <= 0.0) {
 #pragma unroll
             for (int k = 0; k < NV; ++k) F[k] = FR[k] + SR * (Us[k] - UR[k]);
-            return;
+            return true;
         }
         double utLs, uwLs, BtLs, BwLs;
         {
@@ -381,6 +382,13 @@ MHD_HD_INLINE void hlld(const double* UL, const double* UR, double ch, double g,
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = FR[k] + SR * (Us[k] - UR[k]) + SRs * (Uss[k] - Us[k]);
     }
+    return true;
+}
+
+// hlld as a whole (the star solver or, where it gives up, HLL).
+template <int DIR>
+MHD_HD_INLINE void hlld(const double* UL, const double* UR, double ch, double g, double* F) {
+    if (!hlld_star<DIR>(UL, UR, ch, g, F)) hll<DIR>(UL, UR, ch, g, F);
 }
 
 template <int DIR>
@@ -439,14 +447,20 @@ MHD_HD_INLINE void glm_overwrite(double* F, const double* UL, const double* UR, 
 template <int DIR, int SOLVER>
 MHD_HD_INLINE void riemann(const double* UL, const double* UR, double ch, double g, double* F) {
     if (SOLVER == HLL) { hll<DIR>(UL, UR, ch, g, F); return; }
-    if (SOLVER == HLLC) hllc<DIR>(UL, UR, ch, g, F);
-    else if (SOLVER == HLLD) hlld<DIR>(UL, UR, ch, g, F);
+    // HLLC / HLLD report a fallback instead of computing HLL themselves, so one
+    // inlined HLL serves every fallback with the reference's outcome: a star
+    // solver that gave up returns hll_flux, which is still checked and, if
+    // finite, overwritten with the GLM flux; a non-finite result becomes HLL
+    // without the overwrite.
+    bool ok = true;
+    if (SOLVER == HLLC) ok = hllc_star<DIR>(UL, UR, ch, g, F);
+    else if (SOLVER == HLLD) ok = hlld_star<DIR>(UL, UR, ch, g, F);
     else force<DIR>(UL, UR, ch, g, F);
-    if (!isfinite(F[RHO]) || !isfinite(F[EN]) || !isfinite(F[BX]) || !isfinite(F[PSI])) {
-        hll<DIR>(UL, UR, ch, g, F);
-        return;
-    }
-    glm_overwrite<DIR>(F, UL, UR, ch);
+    bool overwrite = true;
+    if (ok && (!isfinite(F[RHO]) || !isfinite(F[EN]) || !isfinite(F[BX]) || !isfinite(F[PSI]))) overwrite = false;
+    if (!ok || !overwrite) hll<DIR>(UL, UR, ch, g, F);
+    if (!ok && (!isfinite(F[RHO]) || !isfinite(F[EN]) || !isfinite(F[BX]) || !isfinite(F[PSI]))) overwrite = false;
+    if (overwrite) glm_overwrite<DIR>(F, UL, UR, ch);
 }
 
 // ---------------------------------------------------------------------------

@@ -170,10 +170,10 @@ __device__ __forceinline__ void hll(const Side& L, const Side& R, float ch, floa
 
 // hllc_flux (head/riemann.hpp:122-241)
 template <int DIR>
-__device__ __forceinline__ void hllc(const Side& L, const Side& R, float ch, float g, float* F) {
+__device__ __forceinline__ bool hllc_star(const Side& L, const Side& R, float ch, float g, float* F) {
     const float* VL = L.W();
     const float* VR = R.W();
-    if (!riemann_physical(VL) || !riemann_physical(VR)) { hll<DIR>(L, R, ch, g, F); return; }
+    if (!riemann_physical(VL) || !riemann_physical(VR)) return false;
     const float rhoL = VL[RHO], rhoR = VR[RHO], pL = VL[PP], pR = VR[PP];
     float unL, unR, utL, utR, uwL, uwR, BnL, BnR, BtL, BtR, BwL, BwR;
     rotate<DIR>(VL, unL, utL, uwL, BnL, BtL, BwL);
@@ -181,17 +181,17 @@ __device__ __forceinline__ void hllc(const Side& L, const Side& R, float ch, flo
     const float cfL = fast_speed<DIR>(VL, g), cfR = fast_speed<DIR>(VR, g);
     const float SL = fminf(unL - cfL, unR - cfR);
     const float SR = fmaxf(unL + cfL, unR + cfR);
-    if (SL >= 0.0f) { flux<DIR>(L.U(), VL, ch, F); return; }
-    if (SR <= 0.0f) { flux<DIR>(R.U(), VR, ch, F); return; }
+    if (SL >= 0.0f) { flux<DIR>(L.U(), VL, ch, F); return true; }
+    if (SR <= 0.0f) { flux<DIR>(R.U(), VR, ch, F); return true; }
     const float ptL = pL + 0.5f * (BnL * BnL + BtL * BtL + BwL * BwL);
     const float ptR = pR + 0.5f * (BnR * BnR + BtR * BtR + BwR * BwR);
     const float numerSM = (SR - unR) * rhoR * unR - (SL - unL) * rhoL * unL + ptL - ptR;
     const float denomSM = (SR - unR) * rhoR - (SL - unL) * rhoL;
-    if (fabsf(denomSM) < 1.0e-14f) { hll<DIR>(L, R, ch, g, F); return; }
+    if (fabsf(denomSM) < 1.0e-14f) return false;
     const float SM = numerSM / denomSM;
     const float rhoLs = rhoL * (SL - unL) / (SL - SM);
     const float rhoRs = rhoR * (SR - unR) / (SR - SM);
-    if (rhoLs <= 0.0f || rhoRs <= 0.0f || !both_finite(rhoLs, rhoRs)) { hll<DIR>(L, R, ch, g, F); return; }
+    if (rhoLs <= 0.0f || rhoRs <= 0.0f || !both_finite(rhoLs, rhoRs)) return false;
     const float psiM = 0.5f * (VL[PSI] + VR[PSI]) - 0.5f * ch * (BnR - BnL);
     float Us[NV], Fs[NV];
     if (SM >= 0.0f) {
@@ -209,6 +209,7 @@ __device__ __forceinline__ void hllc(const Side& L, const Side& R, float ch, flo
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = Fs[k] + SR * (Us[k] - R.U()[k]);
     }
+    return true;
 }
 
 // Single-star state of one side (head/riemann.hpp:340-373).
@@ -230,10 +231,10 @@ __device__ __forceinline__ void star_state(float rho, float un, float ut, float 
 
 // hlld_flux (head/riemann.hpp:253-480)
 template <int DIR>
-__device__ __forceinline__ void hlld(const Side& L, const Side& R, float ch, float g, float* F) {
+__device__ __forceinline__ bool hlld_star(const Side& L, const Side& R, float ch, float g, float* F) {
     const float* VL = L.W();
     const float* VR = R.W();
-    if (!riemann_physical(VL) || !riemann_physical(VR)) { hll<DIR>(L, R, ch, g, F); return; }
+    if (!riemann_physical(VL) || !riemann_physical(VR)) return false;
     const float rhoL = VL[RHO], rhoR = VR[RHO], pL = VL[PP], pR = VR[PP];
     float unL, unR, utL, utR, uwL, uwR, BnL, BnR, BtL, BtR, BwL, BwR;
     rotate<DIR>(VL, unL, utL, uwL, BnL, BtL, BwL);
@@ -241,18 +242,18 @@ __device__ __forceinline__ void hlld(const Side& L, const Side& R, float ch, flo
     const float cfL = fast_speed<DIR>(VL, g), cfR = fast_speed<DIR>(VR, g);
     const float SL = fminf(unL - cfL, unR - cfR);
     const float SR = fmaxf(unL + cfL, unR + cfR);
-    if (fabsf(SR - SL) < 1.0e-14f) { hll<DIR>(L, R, ch, g, F); return; }
+    if (fabsf(SR - SL) < 1.0e-14f) return false;
     const float ptL = pL + 0.5f * (BnL * BnL + BtL * BtL + BwL * BwL);
     const float ptR = pR + 0.5f * (BnR * BnR + BtR * BtR + BwR * BwR);
     const float numerSM = (SR - unR) * rhoR * unR - (SL - unL) * rhoL * unL + ptL - ptR;
     const float denomSM = (SR - unR) * rhoR - (SL - unL) * rhoL;
-    if (fabsf(denomSM) < 1.0e-14f) { hll<DIR>(L, R, ch, g, F); return; }
+    if (fabsf(denomSM) < 1.0e-14f) return false;
     const float SM = numerSM / denomSM;
     const float rhoLs = rhoL * (SL - unL) / (SL - SM);
     const float rhoRs = rhoR * (SR - unR) / (SR - SM);
-    if (rhoLs <= 0.0f || rhoRs <= 0.0f || !both_finite(rhoLs, rhoRs)) { hll<DIR>(L, R, ch, g, F); return; }
-    if (SL >= 0.0f) { flux<DIR>(L.U(), VL, ch, F); return; }
-    if (SR <= 0.0f) { flux<DIR>(R.U(), VR, ch, F); return; }
+    if (rhoLs <= 0.0f || rhoRs <= 0.0f || !both_finite(rhoLs, rhoRs)) return false;
+    if (SL >= 0.0f) { flux<DIR>(L.U(), VL, ch, F); return true; }
+    if (SR <= 0.0f) { flux<DIR>(R.U(), VR, ch, F); return true; }
     const float ptstar = ptL + rhoL * (SL - unL) * (SM - unL);
     const float sqL = sqrtf(rhoLs), sqR = sqrtf(rhoRs);
     const float psiM = 0.5f * (VL[PSI] + VR[PSI]) - 0.5f * ch * (BnR - BnL);
@@ -262,7 +263,7 @@ __device__ __forceinline__ void hlld(const Side& L, const Side& R, float ch, flo
     star_state(rhoR, unR, utR, uwR, BnR, BtR, BwR, SR, SM, utRs, uwRs, BtRs, BwRs);
     const bool left = (SM >= 0.0f);
     // the side that owns the face
-    const float rho_ = left ? rhoL : rhoR, un_ = left ? unL : unR, S_ = left ? SL : SR;
+    const float un_ = left ? unL : unR, S_ = left ? SL : SR;
     const float Bn_ = left ? BnL : BnR, pt_ = left ? ptL : ptR;
     const float ut_ = left ? utL : utR, uw_ = left ? uwL : uwR, Bt_ = left ? BtL : BtR, Bw_ = left ? BwL : BwR;
     const float uts = left ? utLs : utRs, uws = left ? uwLs : uwRs, Bts = left ? BtLs : BtRs, Bws = left ? BwLs : BwRs;
@@ -280,7 +281,7 @@ __device__ __forceinline__ void hlld(const Side& L, const Side& R, float ch, flo
     if (single) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = Fs[k] + S_ * (Us[k] - Uside[k]);
-        return;
+        return true;
     }
     // double-star state (head/riemann.hpp:375-413)
     const float denom2 = sqL + sqR;
@@ -298,6 +299,7 @@ __device__ __forceinline__ void hlld(const Side& L, const Side& R, float ch, flo
     build_star<DIR>(rhos, SM, utss, uwss, Bn_, Btss, Bwss, Ess, psiM, Uss);
 #pragma unroll
     for (int k = 0; k < NV; ++k) F[k] = Fs[k] + S_ * (Us[k] - Uside[k]) + Sstar * (Uss[k] - Us[k]);
+    return true;
 }
 
 // force_flux (head/riemann.hpp:486-525)
@@ -351,18 +353,28 @@ __device__ __forceinline__ void glm_overwrite(float* F, const Side& L, const Sid
     F[PSI] = ch * ch * Bn_star;
 }
 
-// riemann_flux dispatcher (head/riemann.hpp:568-592)
+__device__ __forceinline__ bool flux_finite(const float* F) {
+    return fmaf(F[RHO], 0.0f, fmaf(F[EN], 0.0f, fmaf(F[BX], 0.0f, F[PSI] * 0.0f))) == 0.0f;
+}
+
+// riemann_flux dispatcher (head/riemann.hpp:568-592).  HLLC and HLLD report a
+// fallback instead of computing HLL themselves, so one inlined HLL serves every
+// fallback: a star-state solver that gave up (the reference's solver then
+// returns hll_flux, which riemann_flux still checks and, if finite, overwrites
+// with the GLM psi / Bn flux) and a non-finite solver result (HLL, returned
+// without the overwrite).
 template <int DIR, int SOLVER>
 __device__ __forceinline__ void riemann(const Side& L, const Side& R, float ch, float g, float* F) {
     if (SOLVER == HLL) { hll<DIR>(L, R, ch, g, F); return; }
-    if (SOLVER == HLLC) hllc<DIR>(L, R, ch, g, F);
-    else if (SOLVER == HLLD) hlld<DIR>(L, R, ch, g, F);
+    bool ok = true;
+    if (SOLVER == HLLC) ok = hllc_star<DIR>(L, R, ch, g, F);
+    else if (SOLVER == HLLD) ok = hlld_star<DIR>(L, R, ch, g, F);
     else force<DIR>(L, R, ch, g, F);
-    if (!(fmaf(F[RHO], 0.0f, fmaf(F[EN], 0.0f, fmaf(F[BX], 0.0f, F[PSI] * 0.0f))) == 0.0f)) {
-        hll<DIR>(L, R, ch, g, F);
-        return;
-    }
-    glm_overwrite<DIR>(F, L, R, ch);
+    bool overwrite = true;
+    if (ok && !flux_finite(F)) overwrite = false;
+    if (!ok || !overwrite) hll<DIR>(L, R, ch, g, F);
+    if (!ok && !flux_finite(F)) overwrite = false;
+    if (overwrite) glm_overwrite<DIR>(F, L, R, ch);
 }
 
 __device__ __forceinline__ float minmod(float a, float b) {
