@@ -64,6 +64,8 @@ template <class PH>
 __global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) batch_y_kernel(const BatchInst* __restrict__ inst,
                                                                const int* __restrict__ first, int n, int parity,
                                                                int seg) {
+    using R = typename PH::Real;
+    __shared__ R carry[PH::kYCarry ? YS_WARPS * YCarry<PH>::kSlots * 32 : 1];
     const int total = __ldg(first + n);
     const bool lead = (threadIdx.x == 0 && threadIdx.y == 0);
     for (int u = blockIdx.x; u < total; u += gridDim.x) {
@@ -83,7 +85,8 @@ __global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) batch_y_kernel(co
         double vmax = 0.0;
         unsigned reverts = 0;
         if (item < strips * inst[k].y_bands)
-            y_segment<PH>(T, inst[k].U, P, dt, ch, damp, strip, T.ng + r0, min(seg, T.ny - r0), vmax, reverts);
+            y_march<PH>(T, inst[k].U, P, dt, ch, damp, strip, T.ng + r0, min(seg, T.ny - r0), vmax, reverts,
+                        carry + threadIdx.y * YCarry<PH>::kSlots * 32);
         y_fold(P, vmax, reverts);
         if (local == 0 && lead) clock_advance(P, dt, ch);
     }

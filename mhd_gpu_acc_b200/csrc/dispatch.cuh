@@ -11,7 +11,7 @@
 namespace mhd {
 
 // Dynamic shared memory opt-in of the TMA y-sweep, once per policy, with the
-// shared-memory carveout at its maximum so that kYBlocks CTAs' rings fit on an SM.
+// shared-memory carveout at its maximum so that kYTBlocks CTAs' rings fit on an SM.
 template <class PH>
 cudaError_t y_tma_setup() {
     static const cudaError_t e = [] {

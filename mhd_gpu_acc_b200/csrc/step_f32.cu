@@ -16,7 +16,13 @@ struct FastPolicy {
     static constexpr int NW = NV;
     static constexpr int NS = 2 * NV;
     static constexpr int kYWarps = 4;   // y-sweep warps per CTA (side by side)
-    static constexpr int kYBlocks = 3;  // y-sweep CTAs per SM the register budget is cut for
+    // y-sweep window in shared memory (y_segment_carried), 4 CTAs per SM (128
+    // registers, no spills).  Measured at 4096^2 (HLLD, van Leer): 0.674 ms,
+    // against 0.702 ms for the register window at 3 CTAs (168 registers) and
+    // 0.729 ms for the shared-memory window at 3 CTAs.
+    static constexpr bool kYCarry = true;
+    static constexpr int kYBlocks = 4;  // y-sweep CTAs per SM the register budget is cut for
+    static constexpr int kYTBlocks = 3; // the same for the TMA-staged y-sweep
     // x-sweep: 4 warps per CTA, 4 CTAs per SM (128 registers).  Measured at
     // 4096^2 (HLLD, van Leer): 0.591 ms, against 0.612 ms for 8 x 2 and 0.651 ms
     // for 4 x 5 (96 registers, spills).

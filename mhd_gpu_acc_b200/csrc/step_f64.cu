@@ -17,7 +17,13 @@ struct ExactPolicy {
     static constexpr int NW = NV;  // primitive values per cell
     static constexpr int NS = NV;  // values per reconstructed side state (U*)
     static constexpr int kYWarps = 4;   // y-sweep warps per CTA (side by side)
+    // y-sweep window in shared memory (y_segment_carried), 2 CTAs per SM.
+    // Measured at 4096^2 (HLLD, van Leer): 2.97 ms, against 3.11 ms for the
+    // register window (255 registers, spills) and 3.06 ms for the shared-memory
+    // window at 3 CTAs (168 registers, spills).
+    static constexpr bool kYCarry = true;
     static constexpr int kYBlocks = 2;  // y-sweep CTAs per SM the register budget is cut for
+    static constexpr int kYTBlocks = 2; // the same for the TMA-staged y-sweep
     // x-sweep: 4 warps per CTA, 3 CTAs per SM (168 registers, a few spilled).
     // Measured at 4096^2 (HLLD, van Leer): 2.29 ms, against 2.65 ms for one CTA
     // of 8 warps (240 registers) and 2.35 ms for 2 warps x 6.

@@ -10,9 +10,10 @@
 //          reconstruction, face flux and update each run once per cell, in
 //          registers, with no shared-memory staging.
 // y-sweep  (Uin -> Uout): one thread per column; each warp marches down a
-//          segment of rows with a sliding register window (W(r-2), W(r-1),
-//          the last right-biased state and the last face flux).  Row loads are
-//          fully coalesced.
+//          segment of rows with a sliding window (W(r-2), W(r-1), the last
+//          right-biased state and the last face flux), held in registers or,
+//          when the policy asks (kYCarry), in per-lane shared-memory slots.
+//          Row loads are fully coalesced.
 //
 // Both sweeps write the complete ghost ring of their output with the
 // reference's copy_ghost_cells + apply_boundary semantics
@@ -311,6 +312,103 @@ __device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out,
     }
 }
 
+// The same march with its loop-carried values -- the two previous primitive
+// rows (a ring indexed by row parity), the last right-biased state and the
+// last face flux -- kept in per-lane shared-memory slots instead of registers.
+// Slot s of a lane is carry[s * 32 + lane]: a warp's access is one
+// conflict-free row and no other thread reads it, so no synchronisation is
+// needed.  Moving these 2*NW + NS + NV values out of the register file lets
+// the sweep run at the x-sweep's register budget (more resident warps) for a
+// few shared-memory loads and stores per cell; values and operation order are
+// those of y_segment, so results are identical.
+template <class PH>
+struct YCarry {
+    static constexpr int kSlots = 2 * PH::NW + PH::NS + NV;
+};
+
+template <class PH>
+__device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGrid& out, const StepParams& P,
+                                                  double dt, double ch, double damp, int strip, int j0, int count,
+                                                  double& vmax, unsigned& reverts, typename PH::Real* carry) {
+    using R = typename PH::Real;
+    const int lane = threadIdx.x & 31;
+    const int ng = in.ng, ib = ng, ie = ng + in.nx;
+    const int x = strip * 32 + lane;
+    const int j1 = j0 + count;
+    const bool active = (x >= ib && x < ie && count > 0);
+    const double g = P.gamma;
+    const double dtd = dt / P.dy;
+    R* const wring = carry + lane;                    // W of row k: slots (k & 1) * NW + [0, NW)
+    R* const rslot = carry + 2 * PH::NW * 32 + lane;  // last right-biased state: NS slots
+    R* const fslot = rslot + PH::NS * 32;             // last face flux: NV slots
+
+    if (active) {
+        typename PH::Prim Wm, Wc, Wp;
+        typename PH::Side Rprev, L, Rt;
+        R F[NV], U[NV];
+        R Unext[NV];
+        load_cell(in, x, j0 - 2, U);
+        load_cell(in, x, j0 - 1, Unext);
+        PH::prim(U, g, Wp.v);
+#pragma unroll
+        for (int k = 0; k < PH::NW; ++k) wring[(((j0 - 2) & 1) * PH::NW + k) * 32] = Wp.v[k];
+        PH::prim(Unext, g, Wp.v);
+#pragma unroll
+        for (int k = 0; k < PH::NW; ++k) wring[(((j0 - 1) & 1) * PH::NW + k) * 32] = Wp.v[k];
+        load_cell(in, x, j0, Unext);
+#pragma unroll 1
+        for (int r = j0; r <= j1 + 1; ++r) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) U[k] = Unext[k];
+            if (r <= j1) load_cell(in, x, r + 1, Unext);  // prefetch the next row
+            R Uc[NV];
+            if (r >= j0 + 2) load_cell(in, x, r - 2, Uc);  // the row updated below
+            PH::prim(U, g, Wp.v);
+            R* const wm = wring + (r & 1) * PH::NW * 32;        // row r - 2, overwritten by row r
+            R* const wc = wring + ((r - 1) & 1) * PH::NW * 32;  // row r - 1
+#pragma unroll
+            for (int k = 0; k < PH::NW; ++k) { Wm.v[k] = wm[k * 32]; Wc.v[k] = wc[k * 32]; }
+#pragma unroll
+            for (int k = 0; k < PH::NW; ++k) wm[k * 32] = Wp.v[k];
+            PH::template recon<1>(Wm, Wc, Wp, dtd, ch, g, L, Rt);  // cell r-1
+            if (r >= j0 + 1) {
+#pragma unroll
+                for (int k = 0; k < PH::NS; ++k) Rprev.v[k] = rslot[k * 32];
+                PH::template face<1>(Rprev, L, ch, g, F);  // face (r-2 | r-1)
+                if (r >= j0 + 2) {
+                    const int yc = r - 2;
+                    R Fprev[NV], Un[NV];
+#pragma unroll
+                    for (int k = 0; k < NV; ++k) Fprev[k] = fslot[k * 32];
+                    reverts += update_cell<R>(Uc, F, Fprev, R(dtd), Un) ? 1u : 0u;
+                    if (near_edge(out, x, yc)) scatter_ghosts<R>(out, x, yc, Un, P.bc);
+                    Un[PSI] = Un[PSI] * R(damp);
+                    store_cell(out, x, yc, Un);
+                    if (P.accumulate) {
+                        const double s = PH::speed(Un, g, ch);
+                        vmax = (vmax < s) ? s : vmax;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < NV; ++k) fslot[k * 32] = F[k];
+            }
+#pragma unroll
+            for (int k = 0; k < PH::NS; ++k) rslot[k * 32] = Rt.v[k];
+        }
+    }
+}
+
+// y_segment or y_segment_carried, as the policy asks (kYCarry).
+template <class PH>
+__device__ __forceinline__ void y_march(const DevGrid& in, const DevGrid& out, const StepParams& P, double dt,
+                                        double ch, double damp, int strip, int j0, int count, double& vmax,
+                                        unsigned& reverts, typename PH::Real* carry) {
+    if constexpr (PH::kYCarry)
+        y_segment_carried<PH>(in, out, P, dt, ch, damp, strip, j0, count, vmax, reverts, carry);
+    else
+        y_segment<PH>(in, out, P, dt, ch, damp, strip, j0, count, vmax, reverts);
+}
+
 // Warp-wide CFL maximum into one atomic (when P.accumulate) and the revert
 // count into the clock.  Called by whole warps.
 __device__ __forceinline__ void y_fold(const StepParams& P, double vmax, unsigned reverts) {
@@ -362,9 +460,12 @@ __global__ void __launch_bounds__(32 * PH::kYWarps, PH::kYBlocks) sweep_y_kernel
     const int strips = y_strips(in);
     const int w = blockIdx.x * PH::kYWarps + threadIdx.y;
     const int r0 = (w / strips) * per;
+    __shared__ R carry[PH::kYCarry ? PH::kYWarps * YCarry<PH>::kSlots * 32 : 1];
     double vmax = 0.0;
     unsigned reverts = 0;
-    if (r0 < in.ny) y_segment<PH>(in, out, P, dt, ch, damp, w % strips, in.ng + r0, min(per, in.ny - r0), vmax, reverts);
+    if (r0 < in.ny)
+        y_march<PH>(in, out, P, dt, ch, damp, w % strips, in.ng + r0, min(per, in.ny - r0), vmax, reverts,
+                    carry + threadIdx.y * YCarry<PH>::kSlots * 32);
     y_fold(P, vmax, reverts);
     if (P.clock && first) clock_advance(P, dt, ch);
 }

@@ -221,7 +221,7 @@ __device__ __forceinline__ void y_band_tma(const CUtensorMap* map, const DevGrid
 }
 
 template <class PH>
-__global__ void __launch_bounds__(32 * YT_WARPS, PH::kYBlocks)
+__global__ void __launch_bounds__(32 * YT_WARPS, PH::kYTBlocks)
     sweep_y_tma_kernel(const __grid_constant__ CUtensorMap map, DevGrid in, DevGrid out, StepParams P, int per) {
     using R = typename PH::Real;
     extern __shared__ __align__(1024) unsigned char yt_smem[];
