@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4096, help="grid side")
     ap.add_argument("--e2e-steps", type=int, default=16)
+    ap.add_argument("--e2e-lanes", type=int, default=2,
+                    help="workspaces (each on its own stream) that take e2e steps in turn")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -333,15 +335,17 @@ def run_ours(a, world, rank, local):
 
     # e2e through the C ABI with pinned FP32 host buffers (the FP32-bulk step's
     # own state format): every step uploads a state, advances it one FP32-bulk
-    # step and downloads the result.  Steps are independent, so two workspaces
-    # on two streams take turns: step k's download overlaps step k+1's upload
-    # (the two copy directions run at once).
+    # step and downloads the result.  Steps are independent, so `e2e_lanes`
+    # workspaces on their own streams take turns: while one lane downloads,
+    # the next uploads (the two copy directions run at once).  Two lanes
+    # already keep both copy directions busy (three and four measured the
+    # same), so the step is bound by the concurrent H2D + D2H rate.
     e2e = None
     if rank == 0 or True:
         lanes = []
         hin = torch.from_numpy(U0.astype(np.float32)).pin_memory()
         a_in = hin.numpy()
-        for _ in range(2):
+        for _ in range(a.e2e_lanes):
             U = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
             T = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
             ws = m.GpuWorkspace()
@@ -355,7 +359,7 @@ def run_ours(a, world, rank, local):
             lanes.append((U, T, ws, s, hout.numpy(), hout))
 
         def e2e_step(k):
-            U, T, ws, _, a_out, _ = lanes[k % 2]
+            U, T, ws, _, a_out, _ = lanes[k % len(lanes)]
             ws.upload_f32(U, a_in)
             ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
             ws.download_f32(U, a_out)
@@ -383,8 +387,9 @@ def run_ours(a, world, rank, local):
         e2e = {"value": world * cells * a.e2e_steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": a.e2e_steps,
                "what": "per step: H2D of the FP32 SoA state (ghosts included) from pinned memory "
-                       "(mhd_upload_f32), one FP32-bulk step (mhd_run), D2H of the state (mhd_download_f32); two "
-                       "workspaces on two streams alternate, so one step's download overlaps the next step's upload"}
+                       "(mhd_upload_f32), one FP32-bulk step (mhd_run), D2H of the state (mhd_download_f32); "
+                       f"{len(lanes)} workspaces on their own streams take steps in turn, so one step's download "
+                       "overlaps the next step's upload"}
 
     cpu = None
     if world == 1 and rank == 0 and not a.no_cpu_baseline:

@@ -487,7 +487,7 @@ __device__ __forceinline__ void reconstruct(const float* Wm, const float* Wc, co
     for (int k = 0; k < NV; ++k) {
         const float a = Wc[k] - Wm[k], b = Wp[k] - Wc[k];
         const float s = (LIMITER == VANLEER) ? vanleer(a, b) : minmod(a, b);
-        W[k] = fma2(make_float2(-0.5f, 0.5f), dup2(s), dup2(Wc[k]));
+        W[k] = make_float2(fmaf(-0.5f, s, Wc[k]), fmaf(0.5f, s, Wc[k]));
     }
     const unsigned active = __activemask();
     bool okL, okR;
