@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0, help="batch workload seed")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--xrpw", type=int, default=8, help="x-sweep rows per warp")
-    ap.add_argument("--yband", type=int, default=32, help="y-sweep rows per warp band")
+    ap.add_argument("--yband", type=int, default=0,
+                    help="y-sweep rows per warp band (0: the precision's default, 24 FP32 / 32 FP64)")
     ap.add_argument("--ystage", type=int, default=0, choices=[0, 1],
                     help="y-sweep rows: 0 per-thread loads, 1 TMA-staged shared-memory boxes")
     return ap.parse_args()
@@ -410,7 +411,7 @@ def run_ours(a, world, rank, local):
                        "solver": "hlld", "limiter": "vanleer", "precision": "fp32-bulk (fp64 low-beta pressure, "
                        "fp64 dt reduction)", "per_gpu": "one independent instance",
                        "l2": "state 604 MB (fp32) / 1.2 GB (fp64) > 126 MB L2; no flush",
-                       "sweep_shape": {"xrpw": a.xrpw, "yband": a.yband,
+                       "sweep_shape": {"xrpw": a.xrpw, "yband": a.yband or "default (24 fp32, 32 fp64)",
                                        "y_rows": "tma-staged" if a.ystage else "per-thread loads"}},
             "fp64": out_fp64,
             "fp32_over_fp64": (v32 / out_fp64["value"]) if out_fp64 else None,

@@ -97,7 +97,7 @@ struct mhd_workspace {
     double ch = 0.0;
     double cr = 0.18;          // head/physics.hpp:39
     int limiter = MHD_LIMITER_MINMOD;
-    int yseg = mhd::kDefaultYBand;  // y-sweep rows per warp band
+    int yseg = mhd::kDefaultYBand;  // y-sweep rows per warp band (0: the precision's default)
     int xrpw = mhd::kDefaultXRpw;  // x-sweep rows per warp
     int ystage = 0;                // y-sweep rows loaded per thread (1: staged by TMA)
     double dx = 0.0, dy = 0.0;     // cell spacing of the step; 0 = from the grid's extent
@@ -430,8 +430,8 @@ int mhd_set_cr(mhd_workspace* ws, double cr) {
 
 int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage) {
     if (!ws) return fail(MHD_ERR_STATE, "mhd_set_sweep_shape: null workspace");
-    if (xrpw < 1 || xrpw > 64 || yband < 1 || yband > 65536 || ystage < 0 || ystage > 1)
-        return fail(MHD_ERR_ARG, "mhd_set_sweep_shape: need 1 <= xrpw <= 64, 1 <= yband <= 65536, ystage 0 or 1");
+    if (xrpw < 1 || xrpw > 64 || yband < 0 || yband > 65536 || ystage < 0 || ystage > 1)
+        return fail(MHD_ERR_ARG, "mhd_set_sweep_shape: need 1 <= xrpw <= 64, 0 <= yband <= 65536, ystage 0 or 1");
     ws->xrpw = xrpw;
     ws->yseg = yband;
     ws->ystage = ystage;

@@ -39,7 +39,7 @@ cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
         sweep_x_kernel<PH><<<gx, bx, 0, st>>>(in, tmp, P, xrpw);
     }
     if (which & 2) {
-        const int per = yband > 0 ? yband : kDefaultYBand;
+        const int per = yband > 0 ? yband : PH::kYBand;
         const long long bands = (tmp.ny + per - 1) / per;
         alignas(64) CUtensorMap map;
         if (ystage == 1 && P.fault &&

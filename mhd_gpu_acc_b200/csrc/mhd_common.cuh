@@ -30,7 +30,7 @@ enum Bc : int { PERIODIC = 0, TRANSMISSIVE = 1, REFLECTING = 2, DIRICHLET = 3 };
 constexpr int MAX_NG = 4;  // ghost layers supported by the kernels (>= 2 needed)
 constexpr int kDefaultXRpw = 8;  // x-sweep rows per warp
 constexpr int kDefaultYSeg = 64; // batched y-sweep rows per warp segment
-constexpr int kDefaultYBand = 32; // single-grid y-sweep: rows per warp band
+constexpr int kDefaultYBand = 0;  // single-grid y-sweep rows per warp band: 0 = the policy's kYBand
 
 struct DevGrid {
     void* data;          // plane 0, element (0, 0)

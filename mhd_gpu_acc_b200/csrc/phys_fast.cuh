@@ -536,5 +536,20 @@ __device__ __forceinline__ double cell_speed(const float* U, float g, double ch)
     return -1.0;
 }
 
+// Folds one updated cell's CFL speed into acc without cell_speed's c_h floor
+// and FP64 arithmetic: the maximum over cells of max(s_x, s_y, c_h) equals
+// max(c_h, maximum over cells of max(s_x, s_y)), so the caller applies the
+// floor once (acc < 0: no cell counted).  Cells cell_speed skips leave acc
+// unchanged; a NaN directional speed counts as c_h, as fmax makes it there.
+__device__ __forceinline__ void fold_cell_speed(const float* U, float g, float& acc) {
+    float W[NV];
+    c2p(U, g, W);
+    if (!(W[RHO] > 0.0f && W[PP] > 0.0f && both_finite(W[RHO], W[PP]))) return;
+    const float a = fabsf(W[PU]) + fast_speed<0>(W, g);
+    const float b = fabsf(W[PV]) + fast_speed<1>(W, g);
+    if (a == INFINITY || b == INFINITY) return;
+    acc = fmaxf(acc, fmaxf(fmaxf(a, b), 0.0f));
+}
+
 }  // namespace fast
 }  // namespace mhd

@@ -23,6 +23,9 @@ struct FastPolicy {
     static constexpr bool kYCarry = true;
     static constexpr int kYBlocks = 4;  // y-sweep CTAs per SM the register budget is cut for
     static constexpr int kYTBlocks = 3; // the same for the TMA-staged y-sweep
+    // Default y band (rows one warp marches).  Measured at 4096^2 (HLLD, van
+    // Leer): 24 rows 0.659 ms, 16 rows 0.664, 32 rows 0.667, 48 rows 0.698.
+    static constexpr int kYBand = 24;
     // x-sweep: 4 warps per CTA, 4 CTAs per SM (128 registers).  Measured at
     // 4096^2 (HLLD, van Leer): 0.591 ms, against 0.612 ms for 8 x 2 and 0.651 ms
     // for 4 x 5 (96 registers, spills).
@@ -45,6 +48,14 @@ struct FastPolicy {
     }
 
     __device__ static double speed(const float* U, double g, double ch) { return fast::cell_speed(U, (float)g, ch); }
+
+    // The y-sweep's running CFL maximum: FP32, floored by c_h once at the end.
+    using SpeedAcc = float;
+    __device__ static SpeedAcc no_speed() { return -1.0f; }
+    __device__ static void fold_speed(const float* U, double g, double, SpeedAcc& acc) {
+        fast::fold_cell_speed(U, (float)g, acc);
+    }
+    __device__ static double speed_of(SpeedAcc acc, double ch) { return acc < 0.0f ? 0.0 : fmax((double)acc, ch); }
 };
 
 cudaError_t launch_step_f32(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,

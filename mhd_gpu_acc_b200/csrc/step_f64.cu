@@ -24,6 +24,9 @@ struct ExactPolicy {
     static constexpr bool kYCarry = true;
     static constexpr int kYBlocks = 2;  // y-sweep CTAs per SM the register budget is cut for
     static constexpr int kYTBlocks = 2; // the same for the TMA-staged y-sweep
+    // Default y band.  Measured at 4096^2 (HLLD, van Leer): 32 rows 2.97 ms,
+    // 24 rows 2.98, 48 rows 2.98, 16 rows 3.07.
+    static constexpr int kYBand = 32;
     // x-sweep: 4 warps per CTA, 3 CTAs per SM (168 registers, a few spilled).
     // Measured at 4096^2 (HLLD, van Leer): 2.29 ms, against 2.65 ms for one CTA
     // of 8 warps (240 registers) and 2.35 ms for 2 warps x 6.
@@ -46,6 +49,15 @@ struct ExactPolicy {
     }
 
     __device__ static double speed(const double* U, double g, double ch) { return exact::cell_speed(U, g, ch); }
+
+    // The y-sweep's running CFL maximum (cell_speed per cell, as the reference).
+    using SpeedAcc = double;
+    __device__ static SpeedAcc no_speed() { return 0.0; }
+    __device__ static void fold_speed(const double* U, double g, double ch, SpeedAcc& acc) {
+        const double s = exact::cell_speed(U, g, ch);
+        acc = (acc < s) ? s : acc;
+    }
+    __device__ static double speed_of(SpeedAcc acc, double) { return acc; }
 };
 
 cudaError_t launch_step_f64(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,

@@ -268,6 +268,7 @@ __device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out,
     const bool active = (x >= ib && x < ie && count > 0);
     const double g = P.gamma;
     const double dtd = dt / P.dy;
+    typename PH::SpeedAcc acc = PH::no_speed();
 
     if (active) {
         typename PH::Prim Wm, Wc, Wp;
@@ -297,10 +298,7 @@ __device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out,
                     if (near_edge(out, x, yc)) scatter_ghosts<R>(out, x, yc, Un, P.bc);
                     Un[PSI] = Un[PSI] * R(damp);
                     store_cell(out, x, yc, Un);
-                    if (P.accumulate) {
-                        const double s = PH::speed(Un, g, ch);
-                        vmax = (vmax < s) ? s : vmax;
-                    }
+                    if (P.accumulate) PH::fold_speed(Un, g, ch, acc);
                 }
 #pragma unroll
                 for (int k = 0; k < NV; ++k) Fprev[k] = F[k];
@@ -309,6 +307,10 @@ __device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out,
             Wm = Wc;
             Wc = Wp;
         }
+    }
+    if (P.accumulate) {
+        const double v = PH::speed_of(acc, ch);
+        vmax = (vmax < v) ? v : vmax;
     }
 }
 
@@ -338,6 +340,7 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
     const bool active = (x >= ib && x < ie && count > 0);
     const double g = P.gamma;
     const double dtd = dt / P.dy;
+    typename PH::SpeedAcc acc = PH::no_speed();
     R* const wring = carry + lane;                    // W of row k: slots (k & 1) * NW + [0, NW)
     R* const rslot = carry + 2 * PH::NW * 32 + lane;  // last right-biased state: NS slots
     R* const fslot = rslot + PH::NS * 32;             // last face flux: NV slots
@@ -384,10 +387,7 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
                     if (near_edge(out, x, yc)) scatter_ghosts<R>(out, x, yc, Un, P.bc);
                     Un[PSI] = Un[PSI] * R(damp);
                     store_cell(out, x, yc, Un);
-                    if (P.accumulate) {
-                        const double s = PH::speed(Un, g, ch);
-                        vmax = (vmax < s) ? s : vmax;
-                    }
+                    if (P.accumulate) PH::fold_speed(Un, g, ch, acc);
                 }
 #pragma unroll
                 for (int k = 0; k < NV; ++k) fslot[k * 32] = F[k];
@@ -395,6 +395,10 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
 #pragma unroll
             for (int k = 0; k < PH::NS; ++k) rslot[k * 32] = Rt.v[k];
         }
+    }
+    if (P.accumulate) {
+        const double v = PH::speed_of(acc, ch);
+        vmax = (vmax < v) ? v : vmax;
     }
 }
 
@@ -437,12 +441,13 @@ __device__ __forceinline__ void clock_advance(const StepParams& P, double dt, do
 }
 
 // The y-sweep's work is `strips` column strips, each cut into row bands of
-// `per` rows (32 by default).  Warp w takes strip w % strips, band w / strips:
-// the warps of a CTA sit side by side on one band and consecutive CTAs walk
-// across the width first, so the resident CTAs cover a narrow window of
-// full-width rows that moves down the grid.  Measured on B200 (4096^2, FP32):
-// 32-row bands 0.72 ms, 64 rows 0.78 ms, 128 rows 0.96 ms, and one wave of
-// ~300-row bands 1.31 ms -- short bands in a moving window keep the segment
+// `per` rows (the policy's kYBand by default).  Warp w takes strip w % strips,
+// band w / strips: the warps of a CTA sit side by side on one band and
+// consecutive CTAs walk across the width first, so the resident CTAs cover a
+// narrow window of full-width rows that moves down the grid.  Measured on B200
+// (4096^2, FP32, register window): 32-row bands 0.72 ms, 64 rows 0.78 ms, 128
+// rows 0.96 ms, and one wave of ~300-row bands 1.31 ms -- short bands in a
+// moving window keep the segment
 // halos and the pages in use shared.
 __host__ __device__ __forceinline__ int y_strips(const DevGrid& g) { return (g.ng + g.nx + 31) / 32; }
 

@@ -219,9 +219,10 @@ class GpuWorkspace:
     def set_cr(self, cr: float) -> None:
         check(load().mhd_set_cr(self._req(), float(cr)), "mhd_set_cr")
 
-    def set_sweep_shape(self, xrpw: int = 8, yband: int = 32, ystage: int = 0) -> None:
-        """Launch shape only: x-sweep rows per warp, y-sweep rows per warp band,
-        y-sweep rows staged by TMA (1) or loaded per thread (0)."""
+    def set_sweep_shape(self, xrpw: int = 8, yband: int = 0, ystage: int = 0) -> None:
+        """Launch shape only: x-sweep rows per warp, y-sweep rows per warp band
+        (0: the precision's default), y-sweep rows staged by TMA (1) or loaded
+        per thread (0)."""
         check(load().mhd_set_sweep_shape(self._req(), int(xrpw), int(yband), int(ystage)), "mhd_set_sweep_shape")
 
     @property
