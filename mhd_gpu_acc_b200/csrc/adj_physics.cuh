@@ -301,7 +301,7 @@ ADJ_HD void hside_scatter(const HSide<R>& l, R* lW, R* lU) {
 template <typename R>
 ADJ_HD void star_tan(const HSide<R>& s, R S, R SM, R& uts, R& uws, R& Bts, R& Bws) {
     const R d = s.rho * (S - s.un) * (S - SM) - s.Bn * s.Bn;
-    if (fabs(d) < R(1e-14)) { uts = s.ut; uws = s.uw; Bts = s.Bt; Bws = s.Bw; return; }
+    if (star_degenerate(d, s.rho, s.un, S, SM, s.Bn)) { uts = s.ut; uws = s.uw; Bts = s.Bt; Bws = s.Bw; return; }
     uts = s.ut - s.Bn * s.Bt * (SM - s.un) / d;
     uws = s.uw - s.Bn * s.Bw * (SM - s.un) / d;
     Bts = s.Bt * (s.rho * (S - s.un) * (S - s.un) - s.Bn * s.Bn) / d;
@@ -312,7 +312,10 @@ template <typename R>
 ADJ_HD void star_tan_adj(const HSide<R>& s, R S, R SM, R luts, R luws, R lBts, R lBws, HSide<R>& ls, R& lS,
                          R& lSM) {
     const R q = S - s.un, d = s.rho * q * (S - SM) - s.Bn * s.Bn;
-    if (fabs(d) < R(1e-14)) { ls.ut += luts; ls.uw += luws; ls.Bt += lBts; ls.Bw += lBws; return; }
+    if (star_degenerate(d, s.rho, s.un, S, SM, s.Bn)) {
+        ls.ut += luts; ls.uw += luws; ls.Bt += lBts; ls.Bw += lBws;
+        return;
+    }
     const R e = SM - s.un, f = s.rho * q * q - s.Bn * s.Bn, id = R(1) / d;
     const R A = luts * s.Bt + luws * s.Bw;  // from -Bn (Bt, Bw) e / d
     const R Bc = lBts * s.Bt + lBws * s.Bw; // from (Bt, Bw) f / d

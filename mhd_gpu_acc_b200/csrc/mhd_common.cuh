@@ -11,6 +11,7 @@
 // vector-load-legal) and the 9 planes can be described by one 3-D tensor map.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -28,6 +29,27 @@ enum Limiter : int { MINMOD = 0, VANLEER = 1 };
 enum Bc : int { PERIODIC = 0, TRANSMISSIVE = 1, REFLECTING = 2, DIRICHLET = 3 };
 
 constexpr int MAX_NG = 4;  // ghost layers supported by the kernels (>= 2 needed)
+
+#ifdef __CUDACC__
+#define MHD_HD_RULE __host__ __device__ __forceinline__
+#else
+#define MHD_HD_RULE inline
+#endif
+
+// Degenerate single-star state of HLLD (head/riemann.hpp:342-345, 354-357):
+// d = rho (S - un)(S - SM) - Bn^2 vanishing.  The reference tests |d| < 1e-14,
+// which FP64 resolves (d's rounding noise is ~1e-16 of its terms).  In FP32 the
+// inputs S, un and SM carry noise of ~1e-7 of their size, so near the
+// degenerate state d is that noise and the star state 1 / noise; FP32-bulk
+// therefore takes the degenerate branch when |d| is within 1e-5 of the size of
+// the terms that form it (NaN stays on the non-degenerate path, whose
+// non-finite flux the dispatcher replaces by HLL, as in FP64).
+constexpr float kStarDegenRel = 1.0e-5f;
+MHD_HD_RULE bool star_degenerate(double d, double, double, double, double, double) { return fabs(d) < 1.0e-14; }
+MHD_HD_RULE bool star_degenerate(float d, float rho, float un, float S, float SM, float Bn) {
+    const float m = fabsf(S) + fabsf(un) + fabsf(SM);
+    return fabsf(d) <= kStarDegenRel * (rho * m * m + Bn * Bn);
+}
 constexpr int kDefaultXRpw = 8;  // x-sweep rows per warp
 constexpr int kDefaultYSeg = 64; // batched y-sweep rows per warp segment
 constexpr int kDefaultYBand = 0;  // single-grid y-sweep rows per warp band: 0 = the policy's kYBand

@@ -212,11 +212,12 @@ __device__ __forceinline__ bool hllc_star(const Side& L, const Side& R, float ch
     return true;
 }
 
-// Single-star state of one side (head/riemann.hpp:340-373).
+// Single-star state of one side (head/riemann.hpp:340-373), with the FP32
+// degeneracy test of star_degenerate.
 __device__ __forceinline__ void star_state(float rho, float un, float ut, float uw, float Bn, float Bt, float Bw,
                                            float S, float SM, float& uts, float& uws, float& Bts, float& Bws) {
     const float d = rho * (S - un) * (S - SM) - Bn * Bn;
-    if (fabsf(d) < 1.0e-14f) {
+    if (star_degenerate(d, rho, un, S, SM, Bn)) {
         uts = ut; uws = uw; Bts = Bt; Bws = Bw;
     } else {
         const float inv_d = 1.0f / d;
