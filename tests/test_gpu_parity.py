@@ -210,6 +210,21 @@ def test_fp32_bulk_accuracy(case, n, solver, limiter, steps, tol):
     assert np.all(np.isfinite(U32))
 
 
+def test_fp32_orszag_tang_4096_reaches_t_end():
+    """FP32-bulk Orszag-Tang 4096^2, HLLD + van Leer, to t_end = 0.5: the run
+    completes with positive density and pressure, and c_h -- the running maximum
+    signal speed -- ends where the FP64 step's does (3.49260, reached by t = 0.40
+    and kept to t_end).  With the reference's absolute HLLD degeneracy test, FP32
+    near-degenerate faces produced spurious star states: c_h 5.7 by t = 0.42,
+    then a collapsed time step."""
+    _, U, info, _ = _device_run(4, 4096, 4096, 2, 1, 0, dtype=F32)
+    assert abs(info.t - 0.5) < 1e-12, (info.status, info.t, info.steps)  # run() raises if the loop stopped
+    assert abs(info.ch - 3.49260) < 0.01 * 3.49260, info.ch
+    rho = U[0, 2:-2, 2:-2]
+    e_int = U[7] - 0.5 * (U[1] ** 2 + U[2] ** 2 + U[3] ** 2) / U[0] - 0.5 * (U[4] ** 2 + U[5] ** 2 + U[6] ** 2)
+    assert rho.min() > 0 and e_int[2:-2, 2:-2].min() > 0
+
+
 def test_aos_round_trip():
     g = Grid2DGPU(13, 9, 2, 0.0, 1.0, 0.0, 1.0, F64)
     rng = np.random.default_rng(3)
