@@ -228,8 +228,13 @@ __global__ void objective_kernel(DevGrid U, const double* target, DevGrid lam, d
     if ((threadIdx.x & 31) == 0) atomicAdd(acc + 3, s);
 }
 
+// Reverse of the CFL speed of the argmax cell (*idx; INT_MAX: none) with weight
+// *lm (the step's combined dt / c_h cotangent, from step_scalars_kernel).
 template <typename R>
-__global__ void speed_adj_kernel(DevGrid U, DevGrid lam, int idx, R g, R lm) {
+__global__ void speed_adj_kernel(DevGrid U, DevGrid lam, const int* idx_p, R g, const double* lm_p) {
+    const int idx = *idx_p;
+    if (idx == INT_MAX) return;
+    const R lm = (R)*lm_p;
     const int j = idx / U.nx + U.ng, i = idx % U.nx + U.ng;
     R u[NV], l[NV];
     load_cell(U, i, j, u);
@@ -238,6 +243,28 @@ __global__ void speed_adj_kernel(DevGrid U, DevGrid lam, int idx, R g, R lm) {
     raw_speed(u, g, &branch);
     raw_speed_adj(u, g, branch, lm, l);
     store_cell(lam, i, j, l);
+}
+
+// Per-step scalars of the reverse pass, on the device so the pass needs no
+// host round trip.  sc: [0, 1] the y-sweep's dt/dy and c_h cotangent sums,
+// [2] sum(lambda_psi * psi / f) of the damping fold, [3, 4] the x-sweep's sums,
+// [5] the c_h floor carry between steps, [6] the weight of the argmax cell.
+// The expressions and their order are the host code's before it moved here
+// (explicit round-to-nearest operations, no contraction).
+__global__ void step_scalars_kernel(double* sc, int* idx, double dt, double ch, double f, double cr, double dx,
+                                    double dy, int new_max) {
+    const double ldt = __dadd_rn(__dadd_rn(__ddiv_rn(sc[3], dx), __ddiv_rn(sc[0], dy)),
+                                 __dmul_rn(__dmul_rn(sc[2], f), __ddiv_rn(-ch, cr)));
+    const double lch = __dadd_rn(__dadd_rn(__dadd_rn(sc[4], sc[1]), __dmul_rn(__dmul_rn(sc[2], f), __ddiv_rn(-dt, cr))),
+                                 sc[5]);
+    const double lm = __dadd_rn(lch, __dmul_rn(ldt, __ddiv_rn(-dt, ch)));
+    if (new_max) {  // this step's maximum set c_h: its argmax cell takes lm
+        sc[6] = lm;
+        sc[5] = 0.0;
+        *idx = INT_MAX;
+    } else {        // the floor c_h,n-1 set this step's maximum: lm carries to step n-1
+        sc[5] = lm;
+    }
 }
 
 __device__ __constant__ int kMX[8] = {1, 0, 1, 1, 2, 0, 2, 1};
@@ -323,6 +350,7 @@ struct mhd_adjoint {
     double* d_acc = nullptr;     // [dt/dx-or-dy, ch, f, J] cotangent / objective sums
     double* d_grad = nullptr;    // 16
     int* d_idx = nullptr;
+    double* d_sc = nullptr;      // 8: per-step scalars of the reverse pass (step_scalars_kernel)
     std::vector<double> dt, ch;  // per step
     bool have_target = false;
 };
@@ -410,24 +438,18 @@ int forward(mhd_adjoint* a, const double* amp, double* J, double* rho_final) {
 }
 
 template <typename R>
-int reverse_step(mhd_adjoint* a, int n, const mhd_grid& Un, const mhd_grid& Un1, mhd_grid& lam_next, mhd_grid& lam_out,
-                 double& carry) {
+int reverse_step(mhd_adjoint* a, int n, const mhd_grid& Un, const mhd_grid& Un1, mhd_grid& lam_next,
+                 mhd_grid& lam_out) {
     cudaStream_t st = nullptr;
     const double dt = a->dt[n], ch = a->ch[n];
     const double f = std::exp(-dt * ch / a->cr) >= 1.0 ? 1.0 : std::exp(-dt * ch / a->cr);
     const double dx = 1.0 / a->nx, dy = 1.0 / a->ny;
-    ACK(cudaMemsetAsync(a->d_acc, 0, sizeof(double) * 3, st));
-    // (a) lambda_V from lambda_{n+1}: ghost columns onto sources, damping, dJ/df
+    double* sc = a->d_sc;
+    ACK(cudaMemsetAsync(sc, 0, sizeof(double) * 5, st));
+    // (a) lambda_V from lambda_{n+1}: ghost columns onto sources, damping, dJ/df (into sc[2])
     mhd::adj::fold_kernel<R><<<mhd::adj::blocks_for((long long)a->nx * a->ny), 256, 0, st>>>(
-        dg(lam_next), dg(a->lamV), dg(Un1), 0, 0, 0, 0, 0, f, a->d_acc);
+        dg(lam_next), dg(a->lamV), dg(Un1), 0, 0, 0, 0, 0, f, sc);
     ACK(cudaGetLastError());
-    double acc_f = 0.0;
-    {
-        double h[3];
-        ACK(cudaMemcpy(h, a->d_acc, sizeof h, cudaMemcpyDeviceToHost));
-        acc_f = h[2];
-    }
-    ACK(cudaMemsetAsync(a->d_acc, 0, sizeof(double) * 2, st));
     // (b) T = X(U^n)
     {
         mhd::StepParams P{};
@@ -437,43 +459,30 @@ int reverse_step(mhd_adjoint* a, int n, const mhd_grid& Un, const mhd_grid& Un1,
                                      : mhd::launch_step_f32(dg(Un), dg(a->T), dg(a->T), P, st, mhd::kDefaultYBand, 1);
         ACK(e);
     }
-    // (c) lambda_T = Y^T lambda_V
+    // (c) lambda_T = Y^T lambda_V (dt/dy and c_h sums into sc[0], sc[1])
     ARC(zero_grid(a->lamT, st));
     ACK(mhd::adj::run_adj_sweep<R>(1, a->limiter, a->solver, dg(a->T), dg(a->lamV), dg(a->lamT), a->gamma, dt / dy, ch,
-                                   a->d_acc, st));
-    double s_y[2];
-    ACK(cudaMemcpy(s_y, a->d_acc, sizeof s_y, cudaMemcpyDeviceToHost));
-    ACK(cudaMemsetAsync(a->d_acc, 0, sizeof(double) * 2, st));
-    // (d) ghost rows of T onto their sources (lamV is free again: reuse it)
+                                   sc, st));
+    // (d) ghost rows of T onto their sources (lamV is free again: reuse it; no sums)
     mhd::adj::fold_kernel<R><<<mhd::adj::blocks_for((long long)a->nx * a->ny), 256, 0, st>>>(
-        dg(a->lamT), dg(a->lamV), dg(a->lamT), 1, 0, 0, 0, 0, -1.0, a->d_acc);
+        dg(a->lamT), dg(a->lamV), dg(a->lamT), 1, 0, 0, 0, 0, -1.0, sc);
     ACK(cudaGetLastError());
-    // (e) lambda_U = X^T lambda_T
+    // (e) lambda_U = X^T lambda_T (sums into sc[3], sc[4])
     ARC(zero_grid(lam_out, st));
     ACK(mhd::adj::run_adj_sweep<R>(0, a->limiter, a->solver, dg(Un), dg(a->lamV), dg(lam_out), a->gamma, dt / dx, ch,
-                                   a->d_acc, st));
-    double s_x[2];
-    ACK(cudaMemcpy(s_x, a->d_acc, sizeof s_x, cudaMemcpyDeviceToHost));
-    // (f) the time step and cleaning speed
-    double ldt = s_x[0] / dx + s_y[0] / dy + acc_f * f * (-ch / a->cr);
-    double lch = s_x[1] + s_y[1] + acc_f * f * (-dt / a->cr) + carry;
-    const double lm = lch + ldt * (-dt / ch);
+                                   sc + 3, st));
+    // (f) the time step and cleaning speed: dt = cfl dmin / c_h with c_h the
+    // larger of this step's maximum speed and the previous c_h
     const double ch_prev = n > 0 ? a->ch[n - 1] : 0.0;
-    carry = 0.0;
-    if (ch > ch_prev) {
-        const int big = INT_MAX;
-        ACK(cudaMemcpy(a->d_idx, &big, sizeof big, cudaMemcpyHostToDevice));
+    const int new_max = ch > ch_prev;
+    mhd::adj::step_scalars_kernel<<<1, 1, 0, st>>>(sc, a->d_idx, dt, ch, f, a->cr, dx, dy, new_max);
+    ACK(cudaGetLastError());
+    if (new_max) {
         const cudaError_t e = f64(a) ? mhd::launch_argmax_f64(dg(Un), a->gamma, ch_prev, ch, a->d_idx, st)
                                      : mhd::launch_argmax_f32(dg(Un), a->gamma, ch_prev, ch, a->d_idx, st);
         ACK(e);
-        int idx = big;
-        ACK(cudaMemcpy(&idx, a->d_idx, sizeof idx, cudaMemcpyDeviceToHost));
-        if (idx != big) {
-            mhd::adj::speed_adj_kernel<R><<<1, 1, 0, st>>>(dg(Un), dg(lam_out), idx, (R)a->gamma, (R)lm);
-            ACK(cudaGetLastError());
-        }
-    } else {
-        carry = lm;  // the floor c_h,n-1 set this step's maximum
+        mhd::adj::speed_adj_kernel<R><<<1, 1, 0, st>>>(dg(Un), dg(lam_out), a->d_idx, (R)a->gamma, sc + 6);
+        ACK(cudaGetLastError());
     }
     return MHD_OK;
 }
@@ -489,14 +498,14 @@ int gradient(mhd_adjoint* a, const double* amp, double* J, double* grad) {
         dg(a->seg[0]), a->d_target, dg(a->lamA), a->d_acc);
     ACK(cudaGetLastError());
     mhd_grid lam_next = a->lamA, lam_cur = a->lamB;
-    double carry = 0.0;
+    ACK(cudaMemsetAsync(a->d_sc, 0, sizeof(double) * 8, st));  // the c_h floor carry starts at zero
     const int nseg = (a->nsteps + a->every - 1) / a->every;
     for (int k = nseg - 1; k >= 0; --k) {
         const int n0 = k * a->every, n1 = std::min(a->nsteps, n0 + a->every);
         ARC(grid_copy(a->seg[0], a->ckpt[k], st));
         for (int n = n0; n < n1; ++n) ARC(fwd_step(a, a->seg[n - n0], a->seg[n - n0 + 1], a->dt[n], a->ch[n]));
         for (int n = n1 - 1; n >= n0; --n) {
-            ARC(reverse_step<R>(a, n, a->seg[n - n0], a->seg[n - n0 + 1], lam_next, lam_cur, carry));
+            ARC(reverse_step<R>(a, n, a->seg[n - n0], a->seg[n - n0 + 1], lam_next, lam_cur));
             std::swap(lam_next, lam_cur);
         }
     }
@@ -543,7 +552,8 @@ int mhd_adjoint_create(int nx, int ny, int dtype, int limiter, double gamma, dou
     if (!rc && (cudaMalloc(&a->d_target, sizeof(double) * (size_t)nx * ny) != cudaSuccess ||
                 cudaMalloc(&a->d_acc, sizeof(double) * 4) != cudaSuccess ||
                 cudaMalloc(&a->d_grad, sizeof(double) * 16) != cudaSuccess ||
-                cudaMalloc(&a->d_idx, sizeof(int)) != cudaSuccess))
+                cudaMalloc(&a->d_idx, sizeof(int)) != cudaSuccess ||
+                cudaMalloc(&a->d_sc, sizeof(double) * 8) != cudaSuccess))
         rc = aerr(MHD_ERR_NOMEM, "mhd_adjoint_create: device buffers");
     if (rc) {
         mhd_adjoint_destroy(a);
@@ -572,6 +582,7 @@ int mhd_adjoint_destroy(mhd_adjoint* a) {
     if (a->d_acc) cudaFree(a->d_acc);
     if (a->d_grad) cudaFree(a->d_grad);
     if (a->d_idx) cudaFree(a->d_idx);
+    if (a->d_sc) cudaFree(a->d_sc);
     delete a;
     return MHD_OK;
 }
