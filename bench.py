@@ -61,6 +61,8 @@ def parse():
                          "relative L1 / Linf per field of every configuration, run to t_end")
     ap.add_argument("--precision-max-n", type=int, default=2048,
                     help="largest Orszag-Tang side of the precision workload (512, 2048, 4096)")
+    ap.add_argument("--precision-cases", default="",
+                    help="comma-separated substrings: run only the precision cases whose names contain one")
     ap.add_argument("--seed", type=int, default=0, help="batch workload seed")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--xrpw", type=int, default=8, help="x-sweep rows per warp")
@@ -669,6 +671,9 @@ def run_precision(a, world, rank, local):
     cases += [("shock_bubble_2048_hllc_500_steps", m.CaseId.ShockBubbleMHD, 2048, 2048, HC, MM, 500),
               ("shock_bubble_2048_hlld_500_steps", m.CaseId.ShockBubbleMHD, 2048, 2048, H, MM, 500),
               ("brio_wu_800x4_hlld_cfl0.8", m.CaseId.BrioWuCFL08, 800, 4, H, MM, 0)]
+    if a.precision_cases:
+        keys = [k for k in a.precision_cases.split(",") if k]
+        cases = [c for c in cases if any(k in c[0] for k in keys)]
     out = {}
     for name, case, nx, ny, solver, lim, max_steps in cases:
         cfg = m.get_n_case_config(case, 1)
