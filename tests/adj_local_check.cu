@@ -28,7 +28,26 @@ static void report(const char* name, double adj, double fd) {
     if (e > 1e-6) std::printf("%-10s adj %.12e fd %.12e rel %.2e\n", name, adj, fd, e);
 }
 
+// HLLD degeneracy rule: FP64 keeps the reference's |d| < 1e-14; FP32 compares
+// |d| with 1e-5 of rho (|S| + |un| + |SM|)^2 + Bn^2 (here 9 + 0.25 = 9.25).
+static bool degeneracy_rule_ok() {
+    bool ok = true;
+    ok &= star_degenerate(1e-15, 1.0, 0.5, 1.5, 1.0, 0.5);
+    ok &= !star_degenerate(1e-13, 1.0, 0.5, 1.5, 1.0, 0.5);
+    ok &= star_degenerate(-1e-15, 1.0, 0.5, 1.5, 1.0, 0.5);
+    ok &= star_degenerate(3e-8f, 1.0f, 0.5f, 1.5f, 1.0f, 0.5f);   // rounding-noise size in FP32
+    ok &= star_degenerate(-9e-5f, 1.0f, 0.5f, 1.5f, 1.0f, 0.5f);  // |d| <= 9.25e-5
+    ok &= !star_degenerate(1e-4f, 1.0f, 0.5f, 1.5f, 1.0f, 0.5f);
+    ok &= star_degenerate(0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f);    // all terms zero
+    ok &= !star_degenerate(std::nanf(""), 1.0f, 0.5f, 1.5f, 1.0f, 0.5f);  // NaN: the non-degenerate path
+    return ok;
+}
+
 int main() {
+    if (!degeneracy_rule_ok()) {
+        std::printf("star_degenerate: a known answer failed\n");
+        return 1;
+    }
     const double g = 5.0 / 3.0, h = 1e-6;
     for (int trial = 0; trial < 200; ++trial) {
         double W[NV], U[NV], d[NV], w[NV];
