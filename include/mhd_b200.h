@@ -274,7 +274,7 @@ int mhd_batch_run(mhd_batch* b, int max_steps, mhd_run_info* info);
 int mhd_batch_get_tuning(const mhd_batch* b, mhd_batch_tuning* t);
 int mhd_batch_set_tuning(mhd_batch* b, const mhd_batch_tuning* t);
 /* Autotuner: times each sweep phase for every candidate launch shape (x rows
- * per warp 2/4/8/16 x 2-4 CTAs per SM; y segment 16/32/64/128 x 2-4 CTAs per
+ * per warp 2/4/8/16 x 2-4 CTAs per SM; y segment 16/24/32/48/64/128 x 2-4 CTAs per
  * SM) on the batch's current states, `reps` launches each, and keeps the
  * fastest.  Leaves the instances one step ahead. */
 int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best);

@@ -332,7 +332,7 @@ int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best_out) {
     mhd_batch_tuning best = b->tune;
     const int xr[] = {2, 4, 8, 16};
     const int xc[] = {2, 3, 4};
-    const int ys[] = {16, 32, 64, 128};
+    const int ys[] = {16, 24, 32, 48, 64, 128};
     const int yc[] = {2, 3, 4};
     auto time_phase = [&](int which, float* ms) -> int {
         BCK(phase(b, 0, which, b->tune, b->stream));  // warm
