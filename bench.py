@@ -189,11 +189,18 @@ def barrier(world: int):
         dist.barrier()
 
 
+# The Orszag-Tang [0,1]^2 configuration: gamma 5/3, CFL 0.4, t_end 0.5, periodic.
+OT_EXTENT, OT_GAMMA, OT_CFL, OT_T_END = (0.0, 1.0, 0.0, 1.0), 5.0 / 3.0, 0.4, 0.5
+
+
 def cpu_reference_run(n: int, steps: int, warmup: int, budget_s: float | None):
-    """The reference's CPU step on this host: returns (per-step seconds list, threads)."""
+    """The reference's CPU step on this host: returns (per-step seconds list, threads).
+
+    Everything on this path -- the initial state included -- comes from the
+    reference build (oracle/_ref/libmhdref.so); this repository's library is
+    not loaded."""
     import numpy as np
 
-    from mhd_gpu_acc_b200 import CaseId, get_n_case_config, initialise
     from oracle.oracle import REF_SO, Reference
 
     if not os.path.exists(REF_SO):
@@ -201,15 +208,14 @@ def cpu_reference_run(n: int, steps: int, warmup: int, budget_s: float | None):
     ref = Reference()
     threads = os.cpu_count() or 1
     ref.set_threads(threads)
-    cfg = get_n_case_config(CaseId.OrszagTangUnit, 1)
-    U = initialise(CaseId.OrszagTangUnit, n, n, 2, cfg.extent)
+    U = ref.initialise_orszag_tang_unit(n, n, 2)
     bc = (0, 0, 0, 0)
     if budget_s is not None:  # size the sample from one probe step
-        rc, k, secs, ch = ref.run_timed(U, 2, cfg.extent, cfg.gamma, cfg.cfl, 2, bc, 1, cfg.t_end)
+        rc, k, secs, ch = ref.run_timed(U, 2, OT_EXTENT, OT_GAMMA, OT_CFL, 2, bc, 1, OT_T_END)
         per = float(secs[0])
         steps = int(max(1, min(steps, budget_s / max(per, 1e-9))))
         warmup = 0
-    rc, k, secs, ch = ref.run_timed(U, 2, cfg.extent, cfg.gamma, cfg.cfl, 2, bc, warmup + steps, cfg.t_end)
+    rc, k, secs, ch = ref.run_timed(U, 2, OT_EXTENT, OT_GAMMA, OT_CFL, 2, bc, warmup + steps, OT_T_END)
     del U
     if rc != 0 or k != warmup + steps:
         return None, threads, f"reference run stopped early (rc {rc}, {k} steps)"
@@ -233,7 +239,8 @@ def run_reference_arm(a, world, rank):
         "warmup": a.warmup, "ms_per_step": 1e3 * tot / len(secs), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (deterministic Orszag-Tang initial data)",
         "config": {"workload": f"orszag_tang_unit_{n}x{n}_hlld_cfl0.4", "nx": n, "ny": n, "solver": "hlld",
-                   "limiter": "minmod", "precision": "fp64", "device": "host cpu (OpenMP)"},
+                   "limiter": "minmod", "limiter_note": "reference has minmod only (no van Leer); same cost class",
+                   "precision": "fp64", "device": "host cpu (OpenMP)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

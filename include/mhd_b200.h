@@ -278,6 +278,10 @@ int mhd_batch_set_tuning(mhd_batch* b, const mhd_batch_tuning* t);
  * SM) on the batch's current states, `reps` launches each, and keeps the
  * fastest.  Leaves the instances one step ahead. */
 int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best);
+/* The autotuner's candidate values: which = 0 x rows per warp, 1 y segment
+ * lengths, 2 CTAs per SM (both phases).  Copies up to cap of them into out (may
+ * be NULL) and returns how many there are (MHD_ERR_ARG for another `which`). */
+int mhd_batch_tune_candidates(int which, int* out, int cap);
 
 /* ---- discrete adjoint (no reference counterpart) ----
  * Gradient of J(a) = 1/2 sum_interior (rho(t_N; a) - rho_target)^2 with respect

@@ -127,6 +127,7 @@ PROTOTYPES = {
     "mhd_batch_get_tuning": (_I, [_P, C.POINTER(mhd_batch_tuning)]),
     "mhd_batch_set_tuning": (_I, [_P, C.POINTER(mhd_batch_tuning)]),
     "mhd_batch_tune": (_I, [_P, _I, C.POINTER(mhd_batch_tuning)]),
+    "mhd_batch_tune_candidates": (_I, [_I, _pi, _I]),
     "mhd_adjoint_create": (_I, [_I, _I, _I, _I, _D, _D, _D, _I, _I, C.POINTER(_P)]),
     "mhd_adjoint_destroy": (_I, [_P]),
     "mhd_adjoint_set_solver": (_I, [_P, _I]),

@@ -109,6 +109,16 @@ class Batch:
         check(load().mhd_batch_tune(self.ptr, int(reps), C.byref(t)), "mhd_batch_tune")
         return t
 
+    @staticmethod
+    def tune_candidates(which: int) -> list[int]:
+        """The autotuner's candidates: 0 x rows per warp, 1 y segment lengths,
+        2 CTAs per SM."""
+        n = load().mhd_batch_tune_candidates(int(which), None, 0)
+        check(min(n, 0), "mhd_batch_tune_candidates")
+        out = (C.c_int * n)()
+        load().mhd_batch_tune_candidates(int(which), C.cast(out, C.POINTER(C.c_int)), n)
+        return list(out)
+
     def get_tuning(self) -> mhd_batch_tuning:
         t = mhd_batch_tuning()
         check(load().mhd_batch_get_tuning(self.ptr, C.byref(t)), "mhd_batch_get_tuning")

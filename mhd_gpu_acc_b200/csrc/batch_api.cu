@@ -66,6 +66,12 @@ struct mhd_batch {
 
 namespace {
 
+// Candidate launch shapes the autotuner times (mhd_batch_tune), exported by
+// mhd_batch_tune_candidates.
+const int kTuneXrpw[] = {2, 4, 8, 16};             // x-sweep rows per warp
+const int kTuneYseg[] = {16, 24, 32, 48, 64, 128};  // y-sweep segment rows
+const int kTuneCtasPerSm[] = {2, 3, 4};             // persistent CTAs per SM, both phases
+
 cudaError_t phase(mhd_batch* b, int parity, int which, const mhd_batch_tuning& t, cudaStream_t st) {
     const int ctas = which == 1 ? t.ctas_x : t.ctas_y;
     return b->dtype == MHD_F64 ? mhd::launch_batch_f64(b->d_inst, b->d_first, b->n, parity, which, b->solver,
@@ -321,6 +327,19 @@ int mhd_batch_run(mhd_batch* b, int max_steps, mhd_run_info* info) {
     return MHD_OK;
 }
 
+int mhd_batch_tune_candidates(int which, int* out, int cap) {
+    const int* src = nullptr;
+    int n = 0;
+    switch (which) {
+        case 0: src = kTuneXrpw; n = (int)(sizeof(kTuneXrpw) / sizeof(int)); break;
+        case 1: src = kTuneYseg; n = (int)(sizeof(kTuneYseg) / sizeof(int)); break;
+        case 2: src = kTuneCtasPerSm; n = (int)(sizeof(kTuneCtasPerSm) / sizeof(int)); break;
+        default: return berr(MHD_ERR_ARG, "mhd_batch_tune_candidates: which must be 0, 1 or 2");
+    }
+    for (int k = 0; out && k < n && k < cap; ++k) out[k] = src[k];
+    return n;
+}
+
 int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best_out) {
     if (!b) return berr(MHD_ERR_STATE, "mhd_batch_tune: null batch");
     if (reps < 1) reps = 3;
@@ -330,10 +349,10 @@ int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best_out) {
     BCK(cudaEventCreate(&e0));
     BCK(cudaEventCreate(&e1));
     mhd_batch_tuning best = b->tune;
-    const int xr[] = {2, 4, 8, 16};
-    const int xc[] = {2, 3, 4};
-    const int ys[] = {16, 24, 32, 48, 64, 128};
-    const int yc[] = {2, 3, 4};
+    const auto& xr = kTuneXrpw;
+    const auto& xc = kTuneCtasPerSm;
+    const auto& ys = kTuneYseg;
+    const auto& yc = kTuneCtasPerSm;
     auto time_phase = [&](int which, float* ms) -> int {
         BCK(phase(b, 0, which, b->tune, b->stream));  // warm
         BCK(cudaEventRecord(e0, b->stream));

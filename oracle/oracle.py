@@ -133,6 +133,8 @@ class Reference:
         lib.ref_case_config.restype = _I
         lib.ref_riemann.argtypes = [_dp, _dp, _I, _I, _D, _D, _dp]
         lib.ref_riemann.restype = None
+        lib.ref_initialise_orszag_tang_unit.argtypes = [_I, _I, _I, _dp]
+        lib.ref_initialise_orszag_tang_unit.restype = _I
         lib.ref_set_threads.argtypes = [_I]
         lib.ref_max_threads.restype = _I
         self.lib = lib
@@ -190,6 +192,15 @@ class Reference:
         out = np.zeros(9)
         self.lib.ref_initial_state(case_id, x, y, out)
         return out
+
+    def initialise_orszag_tang_unit(self, nx: int, ny: int, ng: int = 2):
+        """The Orszag-Tang [0,1]^2 initial state (ghosts hold initial-condition
+        values) built by the reference build alone: its Grid2D cell centres and
+        its prim_to_cons.  Returns the (9, ny + 2 ng, nx + 2 ng) SoA array."""
+        U = np.zeros((9, ny + 2 * ng, nx + 2 * ng))
+        if self.lib.ref_initialise_orszag_tang_unit(nx, ny, ng, U) != 0:
+            raise ValueError((nx, ny, ng))
+        return U
 
     def case_config(self, case_id: int, n: int = 1):
         out = np.zeros(14)

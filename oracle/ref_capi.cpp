@@ -225,6 +225,37 @@ void ref_initial_state(int case_id, double x, double y, double* out9) {
     put9(initial_state_at(static_cast<CaseId>(case_id), x, y), out9);
 }
 
+// The Orszag-Tang vortex on periodic [0,1]^2 (rho = 25/(36 pi), p = 5/(12 pi),
+// v = (-sin 2 pi y, sin 2 pi x, 0), B = B0 (-sin 2 pi y, sin 4 pi x, 0),
+// B0 = 1/sqrt(4 pi), gamma 5/3, psi = 0) -- a configuration the reference does
+// not have -- evaluated at the reference Grid2D's own cell centres
+// (head/cpu/grid_cpu.hpp:54-60, ghosts included) and converted with the
+// reference's prim_to_cons (head/physics.hpp:83-90), so that the reference's
+// CPU step can be driven on this configuration without any other library.
+// U: SoA, 9 planes of (nx + 2 ng) x (ny + 2 ng) doubles.
+int ref_initialise_orszag_tang_unit(int nx, int ny, int ng, double* U) {
+    if (!U || nx < 1 || ny < 1 || ng < 0) return -1;
+    const double pi = 3.14159265358979323846;
+    Grid2D g = make_grid(nx, ny, ng, 0.0, 1.0, 0.0, 1.0);
+    phys::gamma = 5.0 / 3.0;
+    const double rho = 25.0 / (36.0 * pi);
+    const double p = 5.0 / (12.0 * pi);
+    const double B0 = 1.0 / std::sqrt(4.0 * pi);
+    for (int j = 0; j < g.total_ny(); ++j) {
+        const double y = g.y_center(j);
+        for (int i = 0; i < g.total_nx(); ++i) {
+            const double x = g.x_center(i);
+            Primitive V;
+            V.rho = rho; V.u = -std::sin(2.0 * pi * y); V.v = std::sin(2.0 * pi * x); V.w = 0.0;
+            V.Bx = -B0 * std::sin(2.0 * pi * y); V.By = B0 * std::sin(4.0 * pi * x); V.Bz = 0.0;
+            V.p = p; V.psi = 0.0;
+            g(i, j) = phys::prim_to_cons(V);
+        }
+    }
+    grid_to_soa(g, U);
+    return 0;
+}
+
 // get_n_case_config (src/test_cases.cpp:275-282): grid and physics scalars.
 // out: nx, ny, ng (as doubles), x_min, x_max, y_min, y_max, cfl, t_end, gamma,
 // bc[4] (as doubles)  -> 14 values.

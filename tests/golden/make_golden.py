@@ -14,7 +14,7 @@ Outputs (committed):
                   apply_boundary known answers
 
 Usage (needs the reference checkout, i.e. only in the build container):
-    make -C oracle && python tests/golden/make_golden.py
+    MHD_REFERENCE_ROOT=<reference checkout> make -C oracle && python tests/golden/make_golden.py
 """
 from __future__ import annotations
 

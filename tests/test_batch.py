@@ -95,7 +95,12 @@ def test_autotuner_picks_a_valid_shape():
     for i in range(len(descs)):
         batch.init_orszag_tang(i, b0[i], gam[i])
     t = batch.tune(2)
-    assert t.xrpw in (2, 4, 8, 16) and t.yseg in (16, 32, 64, 128) and t.ctas_x > 0 and t.ctas_y > 0
+    per_sm = Batch.tune_candidates(2)
+    import torch
+
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    assert t.xrpw in Batch.tune_candidates(0) and t.yseg in Batch.tune_candidates(1)
+    assert t.ctas_x in [c * nsm for c in per_sm] and t.ctas_y in [c * nsm for c in per_sm]
     got = batch.get_tuning()
     assert (got.xrpw, got.yseg) == (t.xrpw, t.yseg)
     info = batch.run(4)

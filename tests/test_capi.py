@@ -89,3 +89,16 @@ def test_baseline_case_definitions():
     assert np.isclose(S[0, 40, 5], (g + 1) * M * M / ((g - 1) * M * M + 2))
     assert np.isclose(S[0, 2 + 32, 2 + 51], 10.0)
     assert np.allclose(S[5], 2.0 / np.sqrt(4 * np.pi))
+
+
+def test_batch_tune_candidates_exported():
+    """The autotuner's candidate lists come from the library itself (host-only
+    call), so tests and callers cannot drift from what mhd_batch_tune tries."""
+    from mhd_gpu_acc_b200.batch import Batch
+
+    assert Batch.tune_candidates(0) == [2, 4, 8, 16]
+    assert Batch.tune_candidates(1) == [16, 24, 32, 48, 64, 128]
+    assert Batch.tune_candidates(2) == [2, 3, 4]
+    from mhd_gpu_acc_b200 import load
+
+    assert load().mhd_batch_tune_candidates(7, None, 0) < 0

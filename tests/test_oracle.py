@@ -126,3 +126,32 @@ def test_oracle_no_speed_error(oracle):
     U = np.zeros((9, 8, 8))
     rc, dt, ch = oracle.compute_dt(U, 2, 0.1, 0.1, 5.0 / 3.0, 0.4, 0.0)
     assert rc == -1
+
+
+@pytest.mark.parametrize("nx,ny,ng", [(64, 48, 2), (33, 17, 3)])
+def test_reference_side_orszag_tang_unit_initial_state(ref, nx, ny, ng):
+    """The [0,1]^2 Orszag-Tang state built by the reference build alone (its
+    Grid2D cell centres and prim_to_cons) equals this library's initial data
+    bit for bit, so the reference arm of the benchmark needs no other library."""
+    cfg = get_n_case_config(4, 1)
+    np.testing.assert_array_equal(ref.initialise_orszag_tang_unit(nx, ny, ng), initialise(4, nx, ny, ng, cfg.extent))
+
+
+def test_reference_arm_loads_only_the_reference_build(ref):
+    """bench.py's reference leg (the timed CPU baseline) maps no library of this
+    repository's package: the initial state, the step and the timing all come
+    from oracle/_ref."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys; sys.path.insert(0, %r); import bench\n"
+            "secs, threads, err = bench.cpu_reference_run(32, 2, 1, None)\n"
+            "assert err is None and len(secs) == 2, err\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libmhdref.so' in maps\n"
+            "assert 'libmhd_b200' not in maps, 'the repository library was loaded'\n"
+            "assert 'mhd_gpu_acc_b200' not in sys.modules\n" % root)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
