@@ -116,6 +116,14 @@ int mhd_set_cr(mhd_workspace* ws, double cr);
  * (same results; on B200 at 4096^2 FP32 the staged sweep measured 0.81 ms
  * against 0.72 ms). */
 int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage);
+/* Limit, in nanoseconds of the GPU's global timer, of each wait of the
+ * TMA-staged y-sweep (ystage 1) for a box of rows to land; 0 restores the
+ * default of 2 s.  A wait that runs out stops the sweep: the CTA waits (with
+ * the full 2 s limit) for the copies it has in flight, the step's output is
+ * left incomplete, and the next synchronising call on the workspace
+ * (mhd_compute_dt, mhd_synchronize, mhd_run ...) returns MHD_ERR_TIMEOUT.
+ * Setting a limit of a few nanoseconds makes that path run on purpose (tests). */
+int mhd_set_tma_wait_limit(mhd_workspace* ws, unsigned long long ns);
 /* Cell spacing the step and compute_dt use instead of the grid's
  * (x_max - x_min) / nx and (y_max - y_min) / ny; (0, 0) restores those.  A slab
  * of a larger grid takes the global spacing, so that its steps equal the
@@ -161,8 +169,9 @@ int mhd_apply_boundary(mhd_workspace* ws, mhd_grid* g, const int* bc);
  * (9 planes of pitch x (ny+2ng) elements, pitch = nx+2ng rounded up to 256
  * bytes) are rejected with MHD_ERR_ARG.  The array's device address is looked
  * up on the first call on each device (make that call before any stream
- * capture).  All calls share the array: calls that can overlap on the GPU race
- * and must be serialised by the caller.  gamma, ch and cr are the values a
+ * capture) and kept until exit, so the device must not be reset between calls.
+ * All calls share the array: calls that can overlap on the GPU race and must
+ * be serialised by the caller.  gamma, ch and cr are the values a
  * workspace would hold; `stream` is a cudaStream_t (NULL = legacy default). */
 #define MHD_NOALLOC_SCRATCH_BYTES (32u << 20)
 int mhd_advance_noalloc(const mhd_grid* Uold, mhd_grid* Unew, double gamma, double ch, double cr, double dt,
@@ -223,6 +232,15 @@ int mhd_initialise(int case_id, int nx, int ny, int ng, double x_min, double x_m
 /* riemann_flux with explicit c_h (head/riemann.hpp:568-592) on one face, on the
  * host, FP64: the functions the FP64 kernels run.  dir 0 = x, 1 = y. */
 int mhd_riemann_flux(const double* UL, const double* UR, int dir, int solver, double ch, double gamma, double* F);
+/* riemann_flux (head/riemann.hpp:568-592) of n independent faces on the GPU,
+ * with the sweep kernels' own solver functions of the given precision:
+ * MHD_F64 (the FP64 step's, bit-equal to mhd_riemann_flux) or MHD_F32 (the
+ * FP32-bulk step's: inputs rounded to FP32, cons->prim with the flagged FP64
+ * pressure branch, FP32 HLLD degeneracy rule).  UL, UR and F are DEVICE arrays
+ * of n x 9 doubles (face k's conserved states / flux at [9k, 9k+9)).  Runs on
+ * the workspace's stream (ws NULL: legacy stream, synchronous). */
+int mhd_riemann_flux_device(mhd_workspace* ws, int dtype, long long n, const double* UL, const double* UR, int dir,
+                            int solver, double ch, double gamma, double* F);
 
 /* Initial data of case_id evaluated on the device at every cell centre of g
  * (ghosts included), without a host array.  Agrees with mhd_initialise to the

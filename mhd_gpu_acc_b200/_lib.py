@@ -96,6 +96,7 @@ PROTOTYPES = {
     "mhd_set_limiter": (_I, [_P, _I]),
     "mhd_set_cr": (_I, [_P, _D]),
     "mhd_set_sweep_shape": (_I, [_P, _I, _I, _I]),
+    "mhd_set_tma_wait_limit": (_I, [_P, C.c_ulonglong]),
     "mhd_set_spacing": (_I, [_P, _D, _D]),
     "mhd_compute_dt": (_I, [_P, _pg, _D, _pd]),
     "mhd_advance": (_I, [_P, _pg, _pg, _pg, _D, _I, _pi]),
@@ -116,6 +117,7 @@ PROTOTYPES = {
     "mhd_initial_state": (_I, [_I, _D, _D, _pd]),
     "mhd_initialise": (_I, [_I, _I, _I, _I, _D, _D, _D, _D, _P]),
     "mhd_riemann_flux": (_I, [_P, _P, _I, _I, _D, _D, _P]),
+    "mhd_riemann_flux_device": (_I, [_P, _I, C.c_longlong, _P, _P, _I, _I, _D, _D, _P]),
     "mhd_initialise_device": (_I, [_P, _pg, _I]),
     "mhd_initialise_orszag_tang": (_I, [_P, _pg, _D, _D, _P]),
     "mhd_batch_create": (_I, [C.POINTER(mhd_instance_desc), _I, _I, _I, _I, C.POINTER(_P)]),

@@ -89,6 +89,8 @@ int report_error(int code, const char* msg) {
     g_err = msg;
     return code;
 }
+// Lets other translation units count their kernel launches in mhd_launch_count().
+void count_launches(unsigned n) { g_launches += n; }
 }  // namespace mhd
 
 struct mhd_workspace {
@@ -100,6 +102,7 @@ struct mhd_workspace {
     int yseg = mhd::kDefaultYBand;  // y-sweep rows per warp band (0: the precision's default)
     int xrpw = mhd::kDefaultXRpw;  // x-sweep rows per warp
     int ystage = 0;                // y-sweep rows loaded per thread (1: staged by TMA)
+    unsigned long long tma_wait_ns = 0;  // limit of each wait for a TMA-staged box (0: 2 s)
     double dx = 0.0, dy = 0.0;     // cell spacing of the step; 0 = from the grid's extent
     int nsm = 148;
     cudaStream_t stream = nullptr;
@@ -165,6 +168,7 @@ mhd::StepParams base_params(const mhd_workspace* ws, const mhd_grid* g, int solv
     P.any_dirichlet = (bc[0] == MHD_BC_DIRICHLET || bc[1] == MHD_BC_DIRICHLET || bc[2] == MHD_BC_DIRICHLET ||
                        bc[3] == MHD_BC_DIRICHLET);
     P.fault = ws->d_fault;
+    P.tma_wait_ns = ws->tma_wait_ns;
     return P;
 }
 
@@ -438,6 +442,12 @@ int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage) {
     return MHD_OK;
 }
 
+int mhd_set_tma_wait_limit(mhd_workspace* ws, unsigned long long ns) {
+    if (!ws) return fail(MHD_ERR_STATE, "mhd_set_tma_wait_limit: null workspace");
+    ws->tma_wait_ns = ns;
+    return MHD_OK;
+}
+
 int mhd_set_spacing(mhd_workspace* ws, double dx, double dy) {
     if (!ws) return fail(MHD_ERR_STATE, "mhd_set_spacing: null workspace");
     if (!(dx >= 0.0) || !(dy >= 0.0) || (dx > 0.0) != (dy > 0.0))
@@ -544,6 +554,21 @@ int mhd_grid_copy_rows(const mhd_grid* src, int src_row, mhd_grid* dst, int dst_
         char* d = static_cast<char*>(dst->data) + ((size_t)f * dst->plane + (size_t)dst_row * dst->pitch) * e;
         CK(cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToDevice, st));
     }
+    return MHD_OK;
+}
+
+int mhd_riemann_flux_device(mhd_workspace* ws, int dtype, long long n, const double* UL, const double* UR, int dir,
+                            int solver, double ch, double gamma, double* F) {
+    if (dtype != MHD_F64 && dtype != MHD_F32) return fail(MHD_ERR_ARG, "mhd_riemann_flux_device: bad dtype %d", dtype);
+    if (n < 0 || (n > 0 && (!UL || !UR || !F))) return fail(MHD_ERR_ARG, "mhd_riemann_flux_device: bad arrays");
+    if (dir != 0 && dir != 1) return fail(MHD_ERR_ARG, "mhd_riemann_flux_device: dir must be 0 (x) or 1 (y)");
+    if (solver < MHD_HLL || solver > MHD_FORCE) return fail(MHD_ERR_ARG, "mhd_riemann_flux_device: bad solver %d", solver);
+    if (n == 0) return MHD_OK;
+    cudaStream_t st = ws ? ws->stream : nullptr;
+    g_launches += 1;
+    CK(dtype == MHD_F64 ? mhd::launch_faces_f64(UL, UR, n, dir, solver, ch, gamma, F, st)
+                        : mhd::launch_faces_f32(UL, UR, n, dir, solver, ch, gamma, F, st));
+    if (!ws) CK(cudaStreamSynchronize(nullptr));
     return MHD_OK;
 }
 

@@ -88,6 +88,54 @@ cudaError_t dispatch_step(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
     return with_policy<POL>(P.solver, P.limiter, go);
 }
 
+// riemann_flux (head/riemann.hpp:568-592) of n independent faces with the
+// sweeps' own solver functions: face k's left / right conserved states are
+// UL[9k..9k+8] / UR[9k..9k+8] (FP64, rounded to the policy's precision), its
+// flux goes to F[9k..9k+8].  No warp-collective operations are involved, so
+// any thread may take any face.
+template <class PH, int DIR>
+__global__ void __launch_bounds__(256) face_flux_kernel(const double* UL, const double* UR, long long n, double ch,
+                                                        double gamma, double* F) {
+    using R = typename PH::Real;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        R uL[NV], uR[NV], f[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) { uL[q] = (R)UL[k * NV + q]; uR[q] = (R)UR[k * NV + q]; }
+        typename PH::Side L, Rs;
+        PH::side(uL, gamma, L);
+        PH::side(uR, gamma, Rs);
+        PH::template face<DIR>(L, Rs, ch, gamma, f);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) F[k * NV + q] = (double)f[q];
+    }
+}
+
+struct FaceLaunch {
+    const double *UL, *UR;
+    long long n;
+    int dir;
+    double ch, gamma;
+    double* F;
+    cudaStream_t st;
+    template <class PH>
+    cudaError_t run() const {
+        long long blocks = (n + 255) / 256;
+        if (blocks > 65535) blocks = 65535;
+        if (blocks < 1) return cudaSuccess;
+        if (dir == 0) face_flux_kernel<PH, 0><<<(unsigned)blocks, 256, 0, st>>>(UL, UR, n, ch, gamma, F);
+        else face_flux_kernel<PH, 1><<<(unsigned)blocks, 256, 0, st>>>(UL, UR, n, ch, gamma, F);
+        return cudaGetLastError();
+    }
+};
+
+template <template <int, int> class POL>
+cudaError_t launch_faces_policy(const double* UL, const double* UR, long long n, int dir, int solver, double ch,
+                                double gamma, double* F, cudaStream_t st) {
+    FaceLaunch go{UL, UR, n, dir, ch, gamma, F, st};
+    return with_policy<POL>(solver, MINMOD, go);
+}
+
 // Smallest linear interior index whose CFL speed (the forward reduction's own
 // per-cell function, floor ch) is m -- exactly for FP64; within 2^-20 relative
 // for FP32, whose code may be contracted differently in another kernel.

@@ -31,6 +31,13 @@ cudaError_t launch_batch_f64(const BatchInst* inst, const int* first, int n, int
 cudaError_t launch_batch_f32(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,
                              int limiter, int xrpw, int yseg, int ctas, cudaStream_t st);
 
+// riemann_flux of n faces (AoS, 9 doubles per face, device memory) with the
+// precision's own solver functions; dir 0 = x, 1 = y.
+cudaError_t launch_faces_f64(const double* UL, const double* UR, long long n, int dir, int solver, double ch,
+                             double gamma, double* F, cudaStream_t st);
+cudaError_t launch_faces_f32(const double* UL, const double* UR, long long n, int dir, int solver, double ch,
+                             double gamma, double* F, cudaStream_t st);
+
 // CFL maximum (floored by ch) folded into *out with atomicMax on the bits.
 cudaError_t launch_max_speed_f64(const DevGrid& g, double gamma, double ch, unsigned long long* out,
                                  cudaStream_t st, int nsm);

@@ -107,6 +107,7 @@ struct StepParams {
     int accumulate;   // y-sweep: also fold the next max signal speed into maxbits
     unsigned long long* max_out;  // explicit mode accumulation target (may be null)
     int* fault;       // ClockStatus bits of a bounded device wait that gave up (may be null)
+    unsigned long long tma_wait_ns;  // limit of each wait for a TMA-staged box (0: the default, 2 s)
 };
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

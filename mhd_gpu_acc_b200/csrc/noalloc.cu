@@ -12,9 +12,11 @@
 // (32 MiB): every GPU that loads the library holds it until the process exits.
 // Its device address is looked up once per device, on the first call made
 // with that device current (cudaGetSymbolAddress); make that first call before
-// any stream capture.  All calls share the one array, so calls whose work can
-// overlap on the GPU (different streams, or different host threads on one
-// device) race on it and must be serialised by the caller.  The x-sweep writes
+// any stream capture.  The address is kept for the life of the process, so the
+// device must not be reset (cudaDeviceReset, or a teardown and re-creation of
+// its primary context) between calls.  All calls share the one array, so calls
+// whose work can overlap on the GPU (different streams, or different host
+// threads on one device) race on it and must be serialised by the caller.  The x-sweep writes
 // every cell of the array that the y-sweep then reads, so nothing has to start
 // at zero.
 #include <cmath>
@@ -26,6 +28,7 @@
 
 namespace mhd {
 int report_error(int code, const char* msg);
+void count_launches(unsigned n);
 }
 
 namespace {
@@ -120,6 +123,7 @@ extern "C" int mhd_advance_noalloc(const mhd_grid* Uold, mhd_grid* Unew, double 
     P.any_dirichlet = (bc[0] == MHD_BC_DIRICHLET || bc[1] == MHD_BC_DIRICHLET || bc[2] == MHD_BC_DIRICHLET ||
                        bc[3] == MHD_BC_DIRICHLET);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    mhd::count_launches(2);  // the x- and the y-sweep
     const cudaError_t e = (Uold->dtype == MHD_F64) ? mhd::launch_step_f64(in, tmp, out, P, st, mhd::kDefaultYBand, 3)
                                                    : mhd::launch_step_f32(in, tmp, out, P, st, mhd::kDefaultYBand, 3);
     if (e != cudaSuccess) return err(MHD_ERR_CUDA, "mhd_advance_noalloc: launch failed (%lld)", (long long)e);

@@ -35,6 +35,12 @@ struct FastPolicy {
     using Side = fast::Side;
 
     __device__ static void prim(const float* U, double g, float* W) { fast::c2p(U, (float)g, W); }
+    // A face-side state made directly from a conserved cell: (U, c2p(U)).
+    __device__ static void side(const float* U, double g, Side& S) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) S.v[k] = U[k];
+        fast::c2p(U, (float)g, S.W());
+    }
 
     template <int DIR>
     __device__ static void recon(const Prim& Wm, const Prim& Wc, const Prim& Wp, double dtd, double ch, double g,
@@ -66,6 +72,11 @@ cudaError_t launch_step_f32(const DevGrid& in, const DevGrid& tmp, const DevGrid
 cudaError_t launch_batch_f32(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,
                              int limiter, int xrpw, int yseg, int ctas, cudaStream_t st) {
     return dispatch_batch<FastPolicy>(inst, first, n, parity, which, solver, limiter, xrpw, yseg, ctas, st);
+}
+
+cudaError_t launch_faces_f32(const double* UL, const double* UR, long long n, int dir, int solver, double ch,
+                             double gamma, double* F, cudaStream_t st) {
+    return launch_faces_policy<FastPolicy>(UL, UR, n, dir, solver, ch, gamma, F, st);
 }
 
 cudaError_t launch_argmax_f32(const DevGrid& g, double gamma, double ch, double m, int* idx, cudaStream_t st) {

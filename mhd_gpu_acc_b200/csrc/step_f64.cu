@@ -36,6 +36,11 @@ struct ExactPolicy {
     struct Side { double v[NV]; };
 
     __device__ static void prim(const double* U, double g, double* W) { exact::c2p(U, g, W); }
+    // A face-side state made directly from a conserved cell (the solvers' input).
+    __device__ static void side(const double* U, double, Side& S) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) S.v[k] = U[k];
+    }
 
     template <int DIR>
     __device__ static void recon(const Prim& Wm, const Prim& Wc, const Prim& Wp, double dtd, double ch, double g,
@@ -68,6 +73,11 @@ cudaError_t launch_step_f64(const DevGrid& in, const DevGrid& tmp, const DevGrid
 cudaError_t launch_batch_f64(const BatchInst* inst, const int* first, int n, int parity, int which, int solver,
                              int limiter, int xrpw, int yseg, int ctas, cudaStream_t st) {
     return dispatch_batch<ExactPolicy>(inst, first, n, parity, which, solver, limiter, xrpw, yseg, ctas, st);
+}
+
+cudaError_t launch_faces_f64(const double* UL, const double* UR, long long n, int dir, int solver, double ch,
+                             double gamma, double* F, cudaStream_t st) {
+    return launch_faces_policy<ExactPolicy>(UL, UR, n, dir, solver, ch, gamma, F, st);
 }
 
 cudaError_t launch_argmax_f64(const DevGrid& g, double gamma, double ch, double m, int* idx, cudaStream_t st) {

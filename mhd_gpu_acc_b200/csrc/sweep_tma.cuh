@@ -15,9 +15,14 @@
 // row r-2 has moved into box k+1); the last of the CTA's warps to release a
 // stage issues the box STAGES later into it, so no warp waits on another's
 // release and no producer warp is needed.  Every wait is bounded by the global
-// timer: a wait that gives up records CLK_TIMEOUT in the fault word (and the
-// clock), waits once more, boundedly, for the copy it was waiting for, and the
-// CTA returns.
+// timer (StepParams::tma_wait_ns, default kTmaWaitNs).  A warp whose wait gives
+// up records CLK_TIMEOUT in the fault word (and the clock) and raises a
+// CTA-wide abort flag in shared memory, so the other warps stop waiting at
+// once instead of each sitting out its own limit on boxes that the aborted
+// warp will never release.  Before the CTA exits, one thread waits (bounded by
+// kTmaWaitNs) for the last box issued into every stage, so no copy can land in
+// the CTA's shared memory after it is gone.  Lanes of a warp agree on every
+// wait's outcome (a vote), so the warp never splits around a __syncwarp.
 //
 // Box coordinates: x = CTA column start (a multiple of 32*YT_WARPS, so 16-byte
 // aligned for both element sizes), row >= 0 (the band starts at ng - 2 or
@@ -74,12 +79,15 @@ __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned pari
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+// Wait for phase `parity` of `bar`, bounded by limit_ns of the global timer and
+// cut short when *abort becomes non-zero (abort may be null); false when it
+// gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, const volatile int* abort,
+                                          unsigned long long limit_ns) {
     if (mbar_test(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (!mbar_test(bar, parity))
-        if (global_ns() - t0 > kTmaWaitNs) return false;
+        if ((abort && *abort) || global_ns() - t0 > limit_ns) return false;
     return true;
 }
 
@@ -112,6 +120,10 @@ __device__ __forceinline__ void y_band_tma(const CUtensorMap* map, const DevGrid
     R* stage = reinterpret_cast<R*>(smem);
     unsigned long long* full = reinterpret_cast<unsigned long long*>(smem + STAGES * yt_stage_bytes<R>());
     int* released = reinterpret_cast<int*>(full + STAGES);
+    int* last_box = released + STAGES;                 // last box issued into each stage (-1: none)
+    volatile int* abort_flag = last_box + STAGES;      // a warp gave up: stop waiting
+    static_assert(STAGES * (8 + 4 + 4) + 4 <= 128, "barrier block exceeds its 128-byte reserve");
+    const unsigned long long wait_ns = P.tma_wait_ns ? P.tma_wait_ns : kTmaWaitNs;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.y;
     const int col = warp * 32 + lane;
@@ -124,11 +136,13 @@ __device__ __forceinline__ void y_band_tma(const CUtensorMap* map, const DevGrid
     const bool lead = (lane == 0 && warp == 0);
 
     if (lead) {
-        for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); released[s] = 0; }
+        for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); released[s] = 0; last_box[s] = -1; }
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         for (int k = 0; k < STAGES && k < nbox; ++k) {
             mbar_expect_tx(&full[k], (unsigned)yt_stage_bytes<R>());
             tma_box(stage + k * STAGE_ELEMS, map, x0, top + k * ROWS, 0, &full[k]);
+            last_box[k] = k;
         }
     }
     __syncthreads();
@@ -144,11 +158,15 @@ __device__ __forceinline__ void y_band_tma(const CUtensorMap* map, const DevGrid
     };
     int ready = -1;   // boxes [0, ready] have landed (as far as this warp knows)
     bool ok = true;
-    auto need = [&](int q) -> bool {           // make box q / ROWS readable
+    auto need = [&](int q) -> bool {           // make box q / ROWS readable (whole warp)
         const int k = q / ROWS;
         while (ready < k) {
             ++ready;
-            if (!mbar_wait(&full[ready % STAGES], (unsigned)((ready / STAGES) & 1))) return false;
+            const bool got = mbar_wait(&full[ready % STAGES], (unsigned)((ready / STAGES) & 1), abort_flag, wait_ns);
+            if (!__all_sync(FULL, got)) {
+                if (lane == 0) *abort_flag = 1;
+                return false;
+            }
         }
         return true;
     };
@@ -164,6 +182,7 @@ __device__ __forceinline__ void y_band_tma(const CUtensorMap* map, const DevGrid
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     mbar_expect_tx(&full[s], (unsigned)yt_stage_bytes<R>());
                     tma_box(stage + s * STAGE_ELEMS, map, x0, top + (k + STAGES) * ROWS, 0, &full[s]);
+                    last_box[s] = k + STAGES;
                 }
             }
         }
@@ -212,11 +231,16 @@ __device__ __forceinline__ void y_band_tma(const CUtensorMap* map, const DevGrid
         // row q-2 was the last read of box (q-2)/ROWS - 1 once q-2 starts a box
         if (q >= 2 + ROWS && (q - 2) % ROWS == 0) release((q - 2) / ROWS - 1);
     }
-    if (!ok) {
-        record_fault(P);
-        // the box this warp gave up on may still be landing: wait for it once
-        // more (bounded) before the CTA's shared memory goes away
-        mbar_wait(&full[ready % STAGES], (unsigned)((ready / STAGES) & 1));
+    if (!ok && lane == 0) record_fault(P);
+    // Drain: every wait above is bounded, so all warps get here.  A box is issued
+    // into a stage only after every warp released the stage's previous box, so
+    // at most the last box of each stage can still be in flight; wait for it
+    // (bounded, with the full limit) before the CTA's shared memory goes away.
+    __syncthreads();
+    if (lead) {
+        for (int s = 0; s < STAGES; ++s)
+            if (last_box[s] >= 0 && !mbar_wait(&full[s], (unsigned)((last_box[s] / STAGES) & 1), nullptr, kTmaWaitNs))
+                record_fault(P);
     }
 }
 

@@ -219,6 +219,10 @@ class GpuWorkspace:
     def set_cr(self, cr: float) -> None:
         check(load().mhd_set_cr(self._req(), float(cr)), "mhd_set_cr")
 
+    def set_tma_wait_limit(self, ns: int) -> None:
+        """Limit (ns) of each wait for a TMA-staged y-sweep box; 0 = the 2 s default."""
+        check(load().mhd_set_tma_wait_limit(self._req(), int(ns)), "mhd_set_tma_wait_limit")
+
     def set_sweep_shape(self, xrpw: int = 8, yband: int = 0, ystage: int = 0) -> None:
         """Launch shape only: x-sweep rows per warp, y-sweep rows per warp band
         (0: the precision's default), y-sweep rows staged by TMA (1) or loaded

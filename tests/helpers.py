@@ -68,3 +68,25 @@ def gpu_driver_loop(U0, nx, ny, ng, extent, gamma, cfl, solver, bc, max_steps=0,
     ch = ws.ch
     ws.destroy()
     return out, t, steps, np.array(dts), ch
+
+
+def device_loop(U0, nx, ny, ng, extent, gamma, cfl, solver, bc, limiter=0, max_steps=0, t_end=1.0, dtype=F64):
+    """The device-resident CUDA-graph driver loop (mhd_run) from the same initial
+    array as gpu_driver_loop.  Returns (U, run_info)."""
+    from mhd_gpu_acc_b200 import GpuWorkspace as _W
+
+    U = Grid2DGPU(nx, ny, ng, *extent, dtype)
+    T = Grid2DGPU(nx, ny, ng, *extent, dtype)
+    U.upload(U0)
+    T.upload(U0)
+    ws = _W()
+    init_gpu_workspace(ws, U)
+    set_gpu_physics_gamma(ws, gamma)
+    set_gpu_physics_ch(ws, 0.0)
+    ws.set_limiter(limiter)
+    info = ws.run(U, T, cfl, t_end, max_steps, solver, bc)
+    out = U.download()
+    ws.destroy()
+    U.release()
+    T.release()
+    return out, info

@@ -121,3 +121,30 @@ def test_torch_autograd_function_gradcheck():
 
     a = torch.tensor(a0, dtype=torch.float64, requires_grad=True)
     assert torch.autograd.gradcheck(OTObjective.apply, (a,), eps=1e-6, atol=1e-6, rtol=1e-3)
+
+
+def _best_of(fn, reps=3):
+    import time
+
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        best = min(best, time.perf_counter() - t0)
+    return best
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [F32, F64])
+def test_gradient_costs_at_most_four_forward_solves(dtype):
+    """The gradient configuration (512^2, 400 steps, HLL + van Leer): the
+    gradient (forward with checkpoints + reverse sweep) costs at most 4x one
+    forward solve, wall time, best of 3 after a warm-up."""
+    adj, a = _problem(512, 400, dtype)
+    adj.forward(a)
+    adj.gradient(a)
+    t_fwd = _best_of(lambda: adj.forward(a))
+    t_grad = _best_of(lambda: adj.gradient(a))
+    print(f"{'FP32' if dtype == F32 else 'FP64'} 512^2 x 400 HLL: forward {t_fwd:.4f} s, gradient {t_grad:.4f} s, "
+          f"ratio {t_grad / t_fwd:.2f}")
+    assert t_grad / t_fwd <= 4.0
