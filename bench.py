@@ -65,7 +65,8 @@ def parse():
                     help="comma-separated substrings: run only the precision cases whose names contain one")
     ap.add_argument("--seed", type=int, default=0, help="batch workload seed")
     ap.add_argument("--instances", type=int, default=256)
-    ap.add_argument("--xrpw", type=int, default=8, help="x-sweep rows per warp")
+    ap.add_argument("--xrpw", type=int, default=8,
+                    help="x-sweep work per warp: one row segment of 128 * xrpw - 4 cells")
     ap.add_argument("--yband", type=int, default=0,
                     help="y-sweep rows per warp band (0: the precision's default, 24 FP32 / 32 FP64)")
     ap.add_argument("--ystage", type=int, default=0, choices=[0, 1],
@@ -327,22 +328,36 @@ def run_ours(a, world, rank, local):
                     "hbm_frac_step": cells * 2 * BYTES_PER_CELL_SWEEP[8] / (res[m.F64]["ms"] / a.steps / 1e3) / 1e9
                     / peaks()[0]}
 
-    # roofline of the dominant FP32 kernel (the slower sweep)
+    # roofline of the dominant FP32 kernel (the slower sweep).  Its bytes are
+    # the HBM roofline's (frac against the measured copy bandwidth), but the
+    # kernel is bound by instruction issue: `issue` gives its warp instructions
+    # per cell (ncu, profiles/traffic.json) and the time those take at one warp
+    # instruction per cycle on every SM sub-partition at the sampled SM clock.
     hbm, kind = peaks()
     mx, my = res[m.F32]["sweeps_ms"]
     dom, dom_ms = ("sweep_y", my) if my >= mx else ("sweep_x", mx)
     alg = cells * BYTES_PER_CELL_SWEEP[4]
     achieved = alg / (dom_ms / 1e3) / 1e9
-    traffic = None
+    traffic, issue = None, None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             tj = json.load(f).get(f"fp32_{dom}")
         if tj:
             traffic = tj["bytes_per_cell"] * cells
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            wi = tj.get("warp_inst_per_cell")
+            clk = (clocks or {}).get("sm_mhz") or 1965.0
+            if wi:
+                sub = 4 * torch.cuda.get_device_properties(local).multi_processor_count
+                ceiling_ms = wi * cells / (sub * clk * 1e6) * 1e3
+                issue = {"warp_inst_per_cell": wi, "thread_inst_per_cell": tj.get("thread_inst_per_cell"),
+                         "issue_ceiling_ms": ceiling_ms, "issue_frac": ceiling_ms / dom_ms, "sm_mhz": clk,
+                         "source": "ncu instruction counts of the same kernel, profiles/traffic.json"}
+    roofline = {"bound": "issue", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": dom, "kernel_ms": dom_ms, "algorithmic_bytes": alg,
-                "peak_kind": kind, "sweep_ms": [mx, my]}
+                "peak_kind": kind, "sweep_ms": [mx, my], "issue": issue,
+                "note": "frac is against the measured HBM copy bandwidth; the kernel is issue-bound (issue.issue_frac "
+                        "= instruction-issue time at one warp instruction per cycle per SM sub-partition / kernel time)"}
 
     # e2e through the C ABI with pinned FP32 host buffers (the FP32-bulk step's
     # own state format): every step uploads a state, advances it one FP32-bulk
@@ -421,8 +436,12 @@ def run_ours(a, world, rank, local):
                        "solver": "hlld", "limiter": "vanleer", "precision": "fp32-bulk (fp64 low-beta pressure, "
                        "fp64 dt reduction)", "per_gpu": "one independent instance",
                        "l2": "state 604 MB (fp32) / 1.2 GB (fp64) > 126 MB L2; no flush",
-                       "sweep_shape": {"xrpw": a.xrpw, "yband": a.yband or "default (24 fp32, 32 fp64)",
-                                       "y_rows": "tma-staged" if a.ystage else "per-thread loads"}},
+                       "sweep_shape": {"xrpw": a.xrpw, "x_segment_cells": 128 * a.xrpw - 4,
+                                       "yband": a.yband or "default (24 fp32, 32 fp64)",
+                                       "y_rows": "tma-staged" if a.ystage else "per-thread loads",
+                                       "y_rows_note": "TMA-staged shared-memory boxes are a launch option "
+                                                      "(--ystage 1); the per-thread loads measured faster for this "
+                                                      "issue-bound kernel"}},
             "fp64": out_fp64,
             "fp32_over_fp64": (v32 / out_fp64["value"]) if out_fp64 else None,
             "rho_rel_l1_fp32_vs_fp64": l1,

@@ -109,7 +109,8 @@ int mhd_set_limiter(mhd_workspace* ws, int limiter);
 /* GLM damping ratio c_r = c_p^2 / c_h (default 0.18, head/physics.hpp:39). */
 int mhd_set_cr(mhd_workspace* ws, double cr);
 /* Launch shape of the sweeps (no reference counterpart; results do not depend
- * on it): x-sweep rows per warp (default 8), the height of the row band one
+ * on it): the x-sweep work per warp, xrpw (default 8; one warp marches a row
+ * segment of 128 * xrpw - 4 cells), the height of the row band one
  * y-sweep warp marches down (0 = the precision's default: 24 rows for FP32,
  * 32 for FP64), and how the y-sweep gets its rows:
  * ystage 0 (default) = per-thread loads, 1 = TMA boxes staged in shared memory
@@ -195,6 +196,55 @@ typedef struct mhd_run_info {
 int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_end, int max_steps, int solver,
             const int* bc, mhd_run_info* info);
 
+/* ---- device-clocked sweeps: the pieces of a step a caller composes itself
+ * (one grid split into y-slabs over several GPUs), with dt, c_h and the psi
+ * damping factor evaluated on the GPU as in mhd_run, so that a step makes no
+ * host round trip (no reference counterpart: the reference reads dt back to
+ * the host every step, src/gpu/solver_gpu.cu:578-605) ----
+ * mhd_clock_start: resets the workspace's device clock (t = 0, no steps) and
+ * puts U's CFL maximum, floored by the workspace's c_h, in clock slot 0;
+ * asynchronous on the workspace stream.  cfl and t_end apply to the sweeps
+ * that follow.
+ * mhd_clock_slot: device address of clock slot `parity` -- the maximum signal
+ * speed as the bit pattern of a non-negative double, which orders like an
+ * unsigned (and a signed) 64-bit integer -- so that a caller can max-reduce it
+ * across slabs or ranks between steps.
+ * mhd_sweep_clocked: one sweep of step n (parity = n % 2) with dt, c_h and
+ * damping from slot parity (a step past t_end or with a bad dt is skipped and
+ * the clock's status says why).  The x-sweep (dir 0) clears slot parity ^ 1;
+ * the y-sweep (dir 1) folds the output's CFL maximum into it.  A y-sweep may
+ * be cut into launches over interior row windows [row0, row0 + nrows)
+ * (nrows 0: every row): MHD_SWEEP_NO_GATHER skips the copy of Dirichlet ghost
+ * cells from the input and MHD_SWEEP_NO_ADVANCE leaves the clock's time and
+ * step count alone, so exactly one launch of a step should do each.
+ * mhd_clock_read: reads the clock into *info, synchronising the workspace
+ * stream, and sets the workspace's c_h to the last step's. */
+#define MHD_SWEEP_NO_GATHER 1
+#define MHD_SWEEP_NO_ADVANCE 2
+int mhd_clock_start(mhd_workspace* ws, const mhd_grid* U, double cfl, double t_end);
+int mhd_clock_slot(mhd_workspace* ws, int parity, void** dptr);
+int mhd_sweep_clocked(mhd_workspace* ws, const mhd_grid* in, mhd_grid* out, int solver, const int* bc, int dir,
+                      int parity, int row0, int nrows, int flags);
+int mhd_clock_read(mhd_workspace* ws, mhd_run_info* info);
+
+/* ---- binary state dump / load (no reference counterpart: the reference has
+ * write-only CSV snapshots, scripts/cpu/main_cpu.cpp:36-91) ----
+ * mhd_state_save writes grid g -- 9 planes in its own precision, ghost cells
+ * included -- with the scalars a resumed run needs to `path` (through
+ * "<path>.tmp" and a rename); mhd_state_load reads such a file into an
+ * allocated grid of the same nx, ny, ng and precision, bit for bit (another
+ * shape or precision: MHD_ERR_ARG).  meta may be NULL (saved as zeros / not
+ * returned).  Both are synchronous on the legacy stream.  A run resumes by
+ * loading the state and setting c_h (mhd_set_ch) to meta.ch. */
+typedef struct mhd_state_meta {
+    double t;          /* simulated time of the state */
+    double ch;         /* GLM c_h carried into the next step */
+    long long steps;   /* steps taken */
+} mhd_state_meta;
+int mhd_state_save(const mhd_grid* g, const char* path, const mhd_state_meta* meta);
+int mhd_state_load(mhd_grid* g, const char* path, mhd_state_meta* meta);
+
+
 /* Measurement aid (no reference counterpart): advances U by nrep device-clock
  * steps like mhd_run, launching each sweep separately between CUDA events on the
  * workspace stream; ms_out[0] / ms_out[1] receive the mean x- / y-sweep kernel
@@ -270,8 +320,9 @@ typedef struct mhd_instance_desc {
     double x_min, x_max, y_min, y_max;
     double gamma, cfl, cr, t_end;
 } mhd_instance_desc;
-/* Launch shape of the batched sweeps: x-sweep rows per warp, y-sweep segment
- * length, persistent CTAs of each phase (0 = default from the SM count). */
+/* Launch shape of the batched sweeps: x-sweep work per warp (xrpw: row
+ * segments of 128 * xrpw - 4 cells), y-sweep segment length, persistent CTAs
+ * of each phase (0 = default from the SM count). */
 typedef struct mhd_batch_tuning {
     int xrpw, yseg, ctas_x, ctas_y;
 } mhd_batch_tuning;
@@ -291,14 +342,15 @@ int mhd_batch_cells(const mhd_batch* b, long long* cells);
 int mhd_batch_run(mhd_batch* b, int max_steps, mhd_run_info* info);
 int mhd_batch_get_tuning(const mhd_batch* b, mhd_batch_tuning* t);
 int mhd_batch_set_tuning(mhd_batch* b, const mhd_batch_tuning* t);
-/* Autotuner: times each sweep phase for every candidate launch shape (x rows
- * per warp 2/4/8/16 x 2-4 CTAs per SM; y segment 16/24/32/48/64/128 x 2-4 CTAs per
- * SM) on the batch's current states, `reps` launches each, and keeps the
- * fastest.  Leaves the instances one step ahead. */
+/* Autotuner: times each sweep phase for every candidate launch shape (x work
+ * per warp xrpw 2/4/8/16 x 2-4 CTAs per SM; y segment 16/24/32/48/64/128 x 2-4
+ * CTAs per SM) on the batch's current states, `reps` launches each, and keeps
+ * the fastest.  Leaves the instances one step ahead. */
 int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best);
-/* The autotuner's candidate values: which = 0 x rows per warp, 1 y segment
- * lengths, 2 CTAs per SM (both phases).  Copies up to cap of them into out (may
- * be NULL) and returns how many there are (MHD_ERR_ARG for another `which`). */
+/* The autotuner's candidate values: which = 0 x work per warp (xrpw), 1 y
+ * segment lengths, 2 CTAs per SM (both phases).  Copies up to cap of them into
+ * out (may be NULL) and returns how many there are (MHD_ERR_ARG for another
+ * `which`). */
 int mhd_batch_tune_candidates(int which, int* out, int cap);
 
 /* ---- discrete adjoint (no reference counterpart) ----

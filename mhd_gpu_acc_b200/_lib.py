@@ -52,6 +52,10 @@ class mhd_run_info(C.Structure):
     ]
 
 
+class mhd_state_meta(C.Structure):
+    _fields_ = [("t", C.c_double), ("ch", C.c_double), ("steps", C.c_longlong)]
+
+
 class mhd_instance_desc(C.Structure):
     _fields_ = [
         ("nx", C.c_int),
@@ -105,6 +109,12 @@ PROTOTYPES = {
     "mhd_max_speed": (_I, [_P, _pg, _pd]),
     "mhd_grid_copy_rows": (_I, [_pg, _I, _pg, _I, _I, _P]),
     "mhd_advance_noalloc": (_I, [_pg, _pg, _D, _D, _D, _D, _I, _I, _pi, _P]),
+    "mhd_clock_start": (_I, [_P, _pg, _D, _D]),
+    "mhd_clock_slot": (_I, [_P, _I, C.POINTER(_P)]),
+    "mhd_sweep_clocked": (_I, [_P, _pg, _pg, _I, _pi, _I, _I, _I, _I, _I]),
+    "mhd_clock_read": (_I, [_P, C.POINTER(mhd_run_info)]),
+    "mhd_state_save": (_I, [_pg, C.c_char_p, C.POINTER(mhd_state_meta)]),
+    "mhd_state_load": (_I, [_pg, C.c_char_p, C.POINTER(mhd_state_meta)]),
     "mhd_run": (_I, [_P, _pg, _pg, _D, _D, _I, _I, _pi, C.POINTER(mhd_run_info)]),
     "mhd_profile_sweeps": (_I, [_P, _pg, _pg, _D, _D, _I, _pi, _I, C.POINTER(C.c_float)]),
     "mhd_upload": (_I, [_P, _pg, _P]),

@@ -111,7 +111,7 @@ class Batch:
 
     @staticmethod
     def tune_candidates(which: int) -> list[int]:
-        """The autotuner's candidates: 0 x rows per warp, 1 y segment lengths,
+        """The autotuner's candidates: 0 x work per warp (xrpw), 1 y segment lengths,
         2 CTAs per SM."""
         n = load().mhd_batch_tune_candidates(int(which), None, 0)
         check(min(n, 0), "mhd_batch_tune_candidates")

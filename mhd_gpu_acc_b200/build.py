@@ -33,6 +33,7 @@ CU_SOURCES = {
     "aux_kernels.cu": [],
     "capi.cu": [],
     "noalloc.cu": [],
+    "state_io.cu": [],
     "compat.cu": ["--fmad=false"],
     "ic_kernels.cu": ["--fmad=false"],
     "batch_api.cu": [],

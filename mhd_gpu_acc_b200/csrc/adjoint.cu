@@ -595,11 +595,13 @@ int mhd_adjoint_set_target(mhd_adjoint* a, const double* rho_target) {
 }
 
 int mhd_adjoint_forward(mhd_adjoint* a, const double* amp16, double* J, double* rho_final) {
+    mhd::NvtxRange nvtx_range("mhd_adjoint_forward");
     if (!a) return aerr(MHD_ERR_STATE, "mhd_adjoint_forward: null handle");
     return forward(a, amp16, J, rho_final);
 }
 
 int mhd_adjoint_gradient(mhd_adjoint* a, const double* amp16, double* J, double* grad16) {
+    mhd::NvtxRange nvtx_range("mhd_adjoint_gradient");
     if (!a || !grad16) return aerr(MHD_ERR_ARG, "mhd_adjoint_gradient: null argument");
     if (!a->have_target) return aerr(MHD_ERR_STATE, "mhd_adjoint_gradient: no target set");
     return f64(a) ? gradient<double>(a, amp16, J, grad16) : gradient<float>(a, amp16, J, grad16);

@@ -2,7 +2,8 @@
 //
 // Each instance (its own grid, gamma, CFL, c_r, boundary types, t_end and
 // device clock) is cut into the same work units the single-grid sweeps use:
-// x units of 28 columns x (BX_WARPS * rpw) rows; y units of YS_WARPS
+// x units of BX_WARPS (row, segment) tasks, segments of x_seg_len(4 * rpw)
+// cells marched by one warp each (x_segment); y units of YS_WARPS
 // consecutive (strip, band) items of an instance, strip-fastest (a strip is 32
 // columns, a band seg rows), as the single-grid y-sweep orders its warps.  The units of all instances
 // form one global list (prefix offsets in `first`, split by phase: first[0..n]
@@ -22,7 +23,7 @@ constexpr int BX_WARPS = 4;  // warps per batched x-sweep CTA
 struct BatchInst {
     DevGrid U, T;
     StepParams P;  // physics, boundary types, t_end and clock of this instance
-    int x_tiles, x_rblocks;
+    int x_segs, x_pad_;      // x-sweep segments per row
     int y_strips, y_bands;   // 32-column strips; bands of seg rows
     int y_units;             // ceil(strips * bands / YS_WARPS)
     int pad_;
@@ -39,10 +40,19 @@ __device__ __forceinline__ int find_instance(const int* first, int n, int u) {
     return lo;
 }
 
+// Dynamic shared memory of the batched x-sweep: one x_segment ring per warp.
+template <class PH>
+constexpr int bx_smem_bytes() { return BX_WARPS * XRing<PH>::kWarpBytes; }
+
 template <class PH>
 __global__ void __launch_bounds__(32 * BX_WARPS, PH::kXBlocks) batch_x_kernel(const BatchInst* __restrict__ inst,
                                                               const int* __restrict__ first, int n, int parity,
                                                               int rpw) {
+    using V = typename Slot16<typename PH::Real>::V;
+    extern __shared__ __align__(16) unsigned char bx_smem[];
+    const int warp = threadIdx.x >> 5;
+    V* ring = reinterpret_cast<V*>(bx_smem + warp * XRing<PH>::kWarpBytes);
+    const int len = x_seg_len(4 * rpw);
     const int total = __ldg(first + n);
     for (int u = blockIdx.x; u < total; u += gridDim.x) {
         const int k = find_instance(first, n, u);
@@ -55,8 +65,12 @@ __global__ void __launch_bounds__(32 * BX_WARPS, PH::kXBlocks) batch_x_kernel(co
             continue;
         }
         if (local == 0 && threadIdx.x == 0) P.clock->maxbits[parity ^ 1] = 0ull;
-        const int tiles = inst[k].x_tiles;
-        x_tile<PH, BX_WARPS>(inst[k].U, inst[k].T, P, dt, ch, local % tiles, local / tiles, rpw);
+        const DevGrid& U = inst[k].U;
+        const long long task = (long long)local * BX_WARPS + warp;
+        if (task < (long long)inst[k].x_segs * U.ny) {  // whole warp
+            const int row = (int)(task % U.ny), c0 = (int)(task / U.ny) * len;
+            x_segment<PH>(U, inst[k].T, P, dt, ch, U.ng + row, c0, min(len, U.nx - c0), ring);
+        }
     }
 }
 
@@ -65,7 +79,7 @@ __global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) batch_y_kernel(co
                                                                const int* __restrict__ first, int n, int parity,
                                                                int seg) {
     using R = typename PH::Real;
-    __shared__ R carry[PH::kYCarry ? YS_WARPS * YCarry<PH>::kSlots * 32 : 1];
+    __shared__ __align__(16) R carry[PH::kYCarry ? YS_WARPS * YCarry<PH>::kSlots * 32 : 1];
     const int total = __ldg(first + n);
     const bool lead = (threadIdx.x == 0 && threadIdx.y == 0);
     for (int u = blockIdx.x; u < total; u += gridDim.x) {
@@ -99,7 +113,18 @@ struct BatchLaunch {
     cudaStream_t st;
     template <class PH>
     cudaError_t run() const {
-        if (which == 1) batch_x_kernel<PH><<<ctas, 32 * BX_WARPS, 0, st>>>(inst, first, n, parity, xrpw);
+        if (which == 1) {
+            static const cudaError_t attr = [] {
+                cudaError_t r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     bx_smem_bytes<PH>());
+                if (r == cudaSuccess)
+                    r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             (int)cudaSharedmemCarveoutMaxShared);
+                return r;
+            }();
+            if (attr != cudaSuccess) return attr;
+            batch_x_kernel<PH><<<ctas, 32 * BX_WARPS, bx_smem_bytes<PH>(), st>>>(inst, first, n, parity, xrpw);
+        }
         else batch_y_kernel<PH><<<ctas, dim3(32, YS_WARPS), 0, st>>>(inst, first + n + 1, n, parity, yseg);
         return cudaGetLastError();
     }

@@ -85,14 +85,14 @@ int build_worklist(mhd_batch* b) {
     b->first.assign(2 * (b->n + 1), 0);
     for (int i = 0; i < b->n; ++i) {
         mhd::BatchInst& I = b->host_inst[i];
-        I.x_tiles = (b->desc[i].nx + mhd::XS_TX - 1) / mhd::XS_TX;
-        const int rows = mhd::BX_WARPS * b->tune.xrpw;
-        I.x_rblocks = (b->desc[i].ny + rows - 1) / rows;
+        const int len = mhd::x_seg_len(4 * b->tune.xrpw);
+        I.x_segs = (b->desc[i].nx + len - 1) / len;
+        I.x_pad_ = 0;
         I.y_strips = (b->desc[i].nx + b->desc[i].ng + 31) / 32;  // strips holding interior columns
         I.y_bands = (b->desc[i].ny + b->tune.yseg - 1) / b->tune.yseg;
         I.y_units = (I.y_strips * I.y_bands + mhd::YS_WARPS - 1) / mhd::YS_WARPS;
         I.pad_ = 0;
-        b->first[i + 1] = b->first[i] + I.x_tiles * I.x_rblocks;
+        b->first[i + 1] = b->first[i] + (int)(((long long)I.x_segs * b->desc[i].ny + mhd::BX_WARPS - 1) / mhd::BX_WARPS);
         b->first[b->n + 1 + i + 1] = b->first[b->n + 1 + i] + I.y_units;
     }
     BCK(cudaMemcpyAsync(b->d_inst, b->host_inst.data(), sizeof(mhd::BatchInst) * b->n, cudaMemcpyHostToDevice,
@@ -260,6 +260,7 @@ int mhd_batch_set_tuning(mhd_batch* b, const mhd_batch_tuning* t) {
 }
 
 int mhd_batch_run(mhd_batch* b, int max_steps, mhd_run_info* info) {
+    mhd::NvtxRange nvtx_range("mhd_batch_run");
     if (!b) return berr(MHD_ERR_STATE, "mhd_batch_run: null batch");
     if (max_steps < 1) return berr(MHD_ERR_ARG, "mhd_batch_run: max_steps must be >= 1");
     int rc = start_clocks(b);
@@ -341,6 +342,7 @@ int mhd_batch_tune_candidates(int which, int* out, int cap) {
 }
 
 int mhd_batch_tune(mhd_batch* b, int reps, mhd_batch_tuning* best_out) {
+    mhd::NvtxRange nvtx_range("mhd_batch_tune");
     if (!b) return berr(MHD_ERR_STATE, "mhd_batch_tune: null batch");
     if (reps < 1) reps = 3;
     int rc = start_clocks(b);

@@ -103,6 +103,8 @@ struct mhd_workspace {
     int xrpw = mhd::kDefaultXRpw;  // x-sweep rows per warp
     int ystage = 0;                // y-sweep rows loaded per thread (1: staged by TMA)
     unsigned long long tma_wait_ns = 0;  // limit of each wait for a TMA-staged box (0: 2 s)
+    double clk_cfl = 0.0, clk_t_end = 0.0;  // of the clock started by mhd_clock_start
+    int clk_started = 0;
     double dx = 0.0, dy = 0.0;     // cell spacing of the step; 0 = from the grid's extent
     int nsm = 148;
     cudaStream_t stream = nullptr;
@@ -458,6 +460,7 @@ int mhd_set_spacing(mhd_workspace* ws, double dx, double dy) {
 }
 
 int mhd_compute_dt(mhd_workspace* ws, const mhd_grid* g, double cfl, double* dt) {
+    mhd::NvtxRange nvtx_range("mhd_compute_dt");
     int rc = check_ws_grid(ws, g, "mhd_compute_dt");
     if (rc) return rc;
     if (!dt) return fail(MHD_ERR_ARG, "mhd_compute_dt: null dt");
@@ -481,6 +484,7 @@ int mhd_compute_dt(mhd_workspace* ws, const mhd_grid* g, double cfl, double* dt)
 
 int mhd_advance(mhd_workspace* ws, const mhd_grid* Uold, mhd_grid* Utmp, mhd_grid* Unew, double dt, int solver,
                 const int* bc) {
+    mhd::NvtxRange nvtx_range("mhd_advance");
     int rc = check_ws_grid(ws, Uold, "mhd_advance(Uold)");
     if (!rc) rc = check_ws_grid(ws, Utmp, "mhd_advance(Utmp)");
     if (!rc) rc = check_ws_grid(ws, Unew, "mhd_advance(Unew)");
@@ -503,6 +507,7 @@ int mhd_advance(mhd_workspace* ws, const mhd_grid* Uold, mhd_grid* Utmp, mhd_gri
 }
 
 int mhd_sweep(mhd_workspace* ws, const mhd_grid* in, mhd_grid* out, double dt, int solver, const int* bc, int dir) {
+    mhd::NvtxRange nvtx_range("mhd_sweep");
     int rc = check_ws_grid(ws, in, "mhd_sweep(in)");
     if (!rc) rc = check_ws_grid(ws, out, "mhd_sweep(out)");
     if (!rc) rc = check_bc(bc);
@@ -607,8 +612,80 @@ static int start_device_loop(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double
     return MHD_OK;
 }
 
+int mhd_clock_start(mhd_workspace* ws, const mhd_grid* U, double cfl, double t_end) {
+    int rc = check_ws_grid(ws, U, "mhd_clock_start");
+    if (rc) return rc;
+    if (!(t_end > 0.0) || !std::isfinite(t_end) || !(cfl > 0.0))
+        return fail(MHD_ERR_ARG, "mhd_clock_start: need finite t_end > 0 and cfl > 0");
+    CK(cudaMemsetAsync(ws->d_max, 0, sizeof(unsigned long long), ws->stream));
+    CK(launch_max(ws, U, ws->stream));
+    g_launches += 1;
+    CK(mhd::launch_clock_init(ws->d_clock, ws->d_max, ws->stream));
+    ws->clk_cfl = cfl;
+    ws->clk_t_end = t_end;
+    ws->clk_started = 1;
+    return MHD_OK;
+}
+
+int mhd_clock_slot(mhd_workspace* ws, int parity, void** dptr) {
+    if (!ws || !ws->d_clock) return fail(MHD_ERR_STATE, "mhd_clock_slot: null workspace");
+    if (!dptr || (parity != 0 && parity != 1)) return fail(MHD_ERR_ARG, "mhd_clock_slot: need parity 0 or 1");
+    *dptr = &ws->d_clock->maxbits[parity];
+    return MHD_OK;
+}
+
+int mhd_sweep_clocked(mhd_workspace* ws, const mhd_grid* in, mhd_grid* out, int solver, const int* bc, int dir,
+                      int parity, int row0, int nrows, int flags) {
+    mhd::NvtxRange nvtx_range("mhd_sweep_clocked");
+    int rc = check_ws_grid(ws, in, "mhd_sweep_clocked(in)");
+    if (!rc) rc = check_ws_grid(ws, out, "mhd_sweep_clocked(out)");
+    if (!rc) rc = check_bc(bc);
+    if (rc) return rc;
+    if (!ws->clk_started) return fail(MHD_ERR_STATE, "mhd_sweep_clocked: no clock (call mhd_clock_start)");
+    if (solver < MHD_HLL || solver > MHD_FORCE) return fail(MHD_ERR_ARG, "mhd_sweep_clocked: bad solver %d", solver);
+    if ((dir != 0 && dir != 1) || (parity != 0 && parity != 1))
+        return fail(MHD_ERR_ARG, "mhd_sweep_clocked: dir and parity must be 0 or 1");
+    if (in->data == out->data) return fail(MHD_ERR_ARG, "mhd_sweep_clocked: in and out must be distinct");
+    if (row0 < 0 || nrows < 0 || row0 + nrows > in->ny || (nrows == 0 && row0 != 0) || (dir == 0 && nrows != 0))
+        return fail(MHD_ERR_ARG, "mhd_sweep_clocked: bad row window %d + %d (y-sweeps only)", row0, nrows);
+    if (flags & ~(MHD_SWEEP_NO_GATHER | MHD_SWEEP_NO_ADVANCE))
+        return fail(MHD_ERR_ARG, "mhd_sweep_clocked: unknown flags %d", flags);
+    mhd::StepParams P = base_params(ws, in, solver, bc);
+    P.cfl = ws->clk_cfl;
+    P.t_end = ws->clk_t_end;
+    P.clock = ws->d_clock;
+    P.accumulate = 1;
+    P.parity = parity;
+    P.row0 = row0;
+    P.nrows = nrows;
+    P.no_gather = (flags & MHD_SWEEP_NO_GATHER) ? 1 : 0;
+    P.no_advance = (flags & MHD_SWEEP_NO_ADVANCE) ? 1 : 0;
+    if (dir == 0) CK(launch_step(in, dev(in), dev(out), dev(out), P, ws->stream, ws->yseg, 1, ws->xrpw, ws->ystage));
+    else CK(launch_step(in, dev(in), dev(in), dev(out), P, ws->stream, ws->yseg, 2, ws->xrpw, ws->ystage));
+    return MHD_OK;
+}
+
+int mhd_clock_read(mhd_workspace* ws, mhd_run_info* info) {
+    if (!ws || !ws->d_clock) return fail(MHD_ERR_STATE, "mhd_clock_read: null workspace");
+    mhd::DevClock hc;
+    CK(cudaMemcpyAsync(&hc, ws->d_clock, sizeof hc, cudaMemcpyDeviceToHost, ws->stream));
+    CK(cudaStreamSynchronize(ws->stream));
+    if (hc.steps > 0) ws->ch = hc.last_ch;
+    if (info) {
+        info->t = hc.t[hc.steps & 1];
+        info->last_dt = hc.last_dt;
+        info->ch = ws->ch;
+        info->steps = hc.steps;
+        info->status = status_code(hc.status);
+        info->fallbacks = hc.flux_fallbacks;
+        info->pad_ = 0;
+    }
+    return check_fault(ws, "mhd_clock_read");
+}
+
 int mhd_profile_sweeps(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_end, int solver,
                        const int* bc, int nrep, float* ms_out) {
+    mhd::NvtxRange nvtx_range("mhd_profile_sweeps");
     if (nrep < 1 || !ms_out) return fail(MHD_ERR_ARG, "mhd_profile_sweeps: need nrep >= 1 and an output");
     mhd::StepParams P;
     int rc = start_device_loop(ws, U, T, cfl, t_end, solver, bc, "mhd_profile_sweeps", &P);
@@ -643,6 +720,7 @@ int mhd_profile_sweeps(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, 
 
 int mhd_run(mhd_workspace* ws, mhd_grid* U, mhd_grid* T, double cfl, double t_end, int max_steps, int solver,
             const int* bc, mhd_run_info* info) {
+    mhd::NvtxRange nvtx_range("mhd_run");
     mhd::StepParams P;
     int rc = start_device_loop(ws, U, T, cfl, t_end, solver, bc, "mhd_run", &P);
     if (rc) return rc;

@@ -25,6 +25,25 @@ cudaError_t y_tma_setup() {
     return e;
 }
 
+// Dynamic shared memory of the x-sweep's rings (kXWarps warps per CTA), with
+// the carveout at its maximum so that kXBlocks CTAs' rings fit on an SM; once
+// per policy, outside any stream capture (the which = 0 set-up launch).
+template <class PH>
+constexpr int x_smem_bytes() { return PH::kXWarps * XRing<PH>::kWarpBytes; }
+
+template <class PH>
+cudaError_t x_setup() {
+    static const cudaError_t e = [] {
+        cudaError_t r = cudaFuncSetAttribute(sweep_x_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             x_smem_bytes<PH>());
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(sweep_x_kernel<PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+        return r;
+    }();
+    return e;
+}
+
 template <class PH>
 cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& out, const StepParams& P,
                           cudaStream_t st, int yband, int which, int xrpw, int ystage) {
@@ -33,14 +52,21 @@ cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
         const cudaError_t e = y_tma_setup<PH>();
         if (e != cudaSuccess) return e;
     }
+    {
+        const cudaError_t e = x_setup<PH>();
+        if (e != cudaSuccess) return e;
+    }
     if (which & 1) {
-        const int rows_per_cta = PH::kXWarps * xrpw;
-        const dim3 bx(32 * PH::kXWarps), gx((in.nx + XS_TX - 1) / XS_TX, (in.ny + rows_per_cta - 1) / rows_per_cta);
-        sweep_x_kernel<PH><<<gx, bx, 0, st>>>(in, tmp, P, xrpw);
+        // xrpw sets the x-sweep work per warp: one row segment of 4 * xrpw chunks of 32 cells
+        const int chunks = 4 * xrpw;
+        const long long segs = (in.nx + x_seg_len(chunks) - 1) / x_seg_len(chunks);
+        const long long ctas = (segs * in.ny + PH::kXWarps - 1) / PH::kXWarps;
+        sweep_x_kernel<PH><<<(unsigned)ctas, 32 * PH::kXWarps, x_smem_bytes<PH>(), st>>>(in, tmp, P, chunks);
     }
     if (which & 2) {
         const int per = yband > 0 ? yband : PH::kYBand;
-        const long long bands = (tmp.ny + per - 1) / per;
+        const int rows = P.nrows > 0 ? P.nrows : tmp.ny - P.row0;  // the interior row window
+        const long long bands = (rows + per - 1) / per;
         alignas(64) CUtensorMap map;
         if (ystage == 1 && P.fault &&
             rows_tensor_map(&map, tmp, (int)sizeof(R), YT_COLS, YTShape<R>::ROWS)) {

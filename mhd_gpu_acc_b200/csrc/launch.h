@@ -3,10 +3,20 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "mhd_common.cuh"
 
 namespace mhd {
+
+// NVTX range over one C-ABI call (visible in Nsight Systems / usable as an
+// ncu --nvtx-include filter); header-only NVTX v3, a no-op without a tool.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // One split step Uin -> Utmp (x) -> Uout (y), reference semantics.
 // which: 1 = x-sweep only, 2 = y-sweep only, 3 = both, 0 = nothing (only the

@@ -108,6 +108,10 @@ struct StepParams {
     unsigned long long* max_out;  // explicit mode accumulation target (may be null)
     int* fault;       // ClockStatus bits of a bounded device wait that gave up (may be null)
     unsigned long long tma_wait_ns;  // limit of each wait for a TMA-staged box (0: the default, 2 s)
+    // y-sweep row window: interior rows [row0, row0 + nrows) (nrows 0: every row)
+    int row0, nrows;
+    int no_gather;    // skip the Dirichlet ghost gather (another launch of the step does it)
+    int no_advance;   // device mode: do not advance the clock (another launch of the step does)
 };
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

@@ -75,6 +75,7 @@ bool valid(const mhd_grid* g) {
 
 extern "C" int mhd_advance_noalloc(const mhd_grid* Uold, mhd_grid* Unew, double gamma, double ch, double cr,
                                    double dt, int solver, int limiter, const int* bc, void* stream) {
+    mhd::NvtxRange nvtx_range("mhd_advance_noalloc");
     if (!valid(Uold) || !valid(Unew)) return err(MHD_ERR_ARG, "mhd_advance_noalloc: invalid grid");
     if (Uold->nx != Unew->nx || Uold->ny != Unew->ny || Uold->ng != Unew->ng || Uold->dtype != Unew->dtype)
         return err(MHD_ERR_ARG, "mhd_advance_noalloc: Uold and Unew differ in shape or precision");

@@ -256,19 +256,20 @@ __device__ __forceinline__ bool hlld_star(const Side& L, const Side& R, float ch
     if (SL >= 0.0f) { flux<DIR>(L.U(), VL, ch, F); return true; }
     if (SR <= 0.0f) { flux<DIR>(R.U(), VR, ch, F); return true; }
     const float ptstar = ptL + rhoL * (SL - unL) * (SM - unL);
-    const float sqL = sqrtf(rhoLs), sqR = sqrtf(rhoRs);
     const float psiM = 0.5f * (VL[PSI] + VR[PSI]) - 0.5f * ch * (BnR - BnL);
     const float signBn = (BnL >= 0.0f) ? 1.0f : -1.0f;
-    float utLs, uwLs, BtLs, BwLs, utRs, uwRs, BtRs, BwRs;
-    star_state(rhoL, unL, utL, uwL, BnL, BtL, BwL, SL, SM, utLs, uwLs, BtLs, BwLs);
-    star_state(rhoR, unR, utR, uwR, BnR, BtR, BwR, SR, SM, utRs, uwRs, BtRs, BwRs);
+    // The side that owns the face (S_M >= 0: left).  Its single-star state is
+    // all a single-star face needs; the other side's star state and square
+    // root are computed only for a double-star face.  The values are those of
+    // the symmetric evaluation (both star states, then a selection).
     const bool left = (SM >= 0.0f);
-    // the side that owns the face
-    const float un_ = left ? unL : unR, S_ = left ? SL : SR;
+    const float rho_ = left ? rhoL : rhoR, un_ = left ? unL : unR, S_ = left ? SL : SR;
     const float Bn_ = left ? BnL : BnR, pt_ = left ? ptL : ptR;
     const float ut_ = left ? utL : utR, uw_ = left ? uwL : uwR, Bt_ = left ? BtL : BtR, Bw_ = left ? BwL : BwR;
-    const float uts = left ? utLs : utRs, uws = left ? uwLs : uwRs, Bts = left ? BtLs : BtRs, Bws = left ? BwLs : BwRs;
-    const float rhos = left ? rhoLs : rhoRs, sq = left ? sqL : sqR;
+    const float rhos = left ? rhoLs : rhoRs;
+    float uts, uws, Bts, Bws;
+    star_state(rho_, un_, ut_, uw_, Bn_, Bt_, Bw_, S_, SM, uts, uws, Bts, Bws);
+    const float sq = sqrtf(rhos);
     const float* Uside = left ? L.U() : R.U();
     const float* Wside = left ? VL : VR;
     const float BdU = Bn_ * un_ + Bt_ * ut_ + Bw_ * uw_;
@@ -277,14 +278,21 @@ __device__ __forceinline__ bool hlld_star(const Side& L, const Side& R, float ch
     float Us[NV], Fs[NV];
     build_star<DIR>(rhos, SM, uts, uws, Bn_, Bts, Bws, Es, psiM, Us);
     flux<DIR>(Uside, Wside, ch, Fs);
-    const float Sstar = left ? SM - fabsf(BnL) / sqL : SM + fabsf(BnR) / sqR;
+    const float Sstar = left ? SM - fabsf(Bn_) / sq : SM + fabsf(Bn_) / sq;
     const bool single = left ? (Sstar >= 0.0f) : (Sstar <= 0.0f);
     if (single) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = Fs[k] + S_ * (Us[k] - Uside[k]);
         return true;
     }
-    // double-star state (head/riemann.hpp:375-413)
+    // double-star state (head/riemann.hpp:375-413): the other side's star state
+    float uto, uwo, Bto, Bwo;
+    star_state(left ? rhoR : rhoL, left ? unR : unL, left ? utR : utL, left ? uwR : uwL, left ? BnR : BnL,
+               left ? BtR : BtL, left ? BwR : BwL, left ? SR : SL, SM, uto, uwo, Bto, Bwo);
+    const float sqo = sqrtf(left ? rhoRs : rhoLs);
+    const float sqL = left ? sq : sqo, sqR = left ? sqo : sq;
+    const float utLs = left ? uts : uto, uwLs = left ? uws : uwo, BtLs = left ? Bts : Bto, BwLs = left ? Bws : Bwo;
+    const float utRs = left ? uto : uts, uwRs = left ? uwo : uws, BtRs = left ? Bto : Bts, BwRs = left ? Bwo : Bws;
     const float denom2 = sqL + sqR;
     float utss = uts, uwss = uws, Btss = Bts, Bwss = Bws, Ess = Es;
     if (fabsf(denom2) >= 1.0e-14f) {
@@ -542,10 +550,26 @@ __device__ __forceinline__ double cell_speed(const float* U, float g, double ch)
 // max(c_h, maximum over cells of max(s_x, s_y)), so the caller applies the
 // floor once (acc < 0: no cell counted).  Cells cell_speed skips leave acc
 // unchanged; a NaN directional speed counts as c_h, as fmax makes it there.
-__device__ __forceinline__ void fold_cell_speed(const float* U, float g, float& acc) {
+//
+// Both directional speeds |u_n| + c_f are at most max(|u|, |v|) + sqrt(a^2 + b^2)
+// (c_f^2 <= a^2 + b^2, sound speed a, Alfven speed b).  A cell whose bound,
+// with a 2^-10 margin over the rounding of either form, stays below
+// max(acc, floor) -- floor being the c_h the caller applies at the end --
+// cannot change the folded result max(acc, c_h), so its two fast speeds (four
+// square roots) are skipped; it still counts as a visited physical cell
+// (acc >= 0).  The result is the one the full evaluation of every cell gives.
+__device__ __forceinline__ void fold_cell_speed(const float* U, float g, float floor, float& acc) {
     float W[NV];
     c2p(U, g, W);
     if (!(W[RHO] > 0.0f && W[PP] > 0.0f && both_finite(W[RHO], W[PP]))) return;
+    {
+        const float s = (g * W[PP] + W[BX] * W[BX] + W[BY] * W[BY] + W[BZ] * W[BZ]) / W[RHO];
+        const float ub = fmaxf(fabsf(W[PU]), fabsf(W[PV])) + sqrtf(s);
+        if (ub * 1.0009765625f < fmaxf(acc, floor)) {
+            acc = fmaxf(acc, 0.0f);
+            return;
+        }
+    }
     const float a = fabsf(W[PU]) + fast_speed<0>(W, g);
     const float b = fabsf(W[PV]) + fast_speed<1>(W, g);
     if (a == INFINITY || b == INFINITY) return;

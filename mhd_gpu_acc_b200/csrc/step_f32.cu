@@ -58,8 +58,8 @@ struct FastPolicy {
     // The y-sweep's running CFL maximum: FP32, floored by c_h once at the end.
     using SpeedAcc = float;
     __device__ static SpeedAcc no_speed() { return -1.0f; }
-    __device__ static void fold_speed(const float* U, double g, double, SpeedAcc& acc) {
-        fast::fold_cell_speed(U, (float)g, acc);
+    __device__ static void fold_speed(const float* U, double g, double ch, SpeedAcc& acc) {
+        fast::fold_cell_speed(U, (float)g, (float)ch, acc);
     }
     __device__ static double speed_of(SpeedAcc acc, double ch) { return acc < 0.0f ? 0.0 : fmax((double)acc, ch); }
 };

@@ -4,11 +4,10 @@
 // kernels per sweep, the psi-damping kernel and the CFL block-max kernel + CUB
 // reduction (src/gpu/solver_gpu.cu:188-251, 265-528; src/gpu/boundary_gpu.cu).
 //
-// x-sweep  (Uin -> Uout): one warp per interior row segment.  Lane l holds the
-//          cell at storage column x0 + l (x0 = ng - 2 + TX*blockIdx.x); the
-//          stencil neighbours are exchanged with warp shuffles, so primitive,
-//          reconstruction, face flux and update each run once per cell, in
-//          registers, with no shared-memory staging.
+// x-sweep  (Uin -> Uout): one warp marches along a row segment in chunks of
+//          32 consecutive cells; the stencil neighbours come from per-warp
+//          shared-memory rings, so primitive, reconstruction, face flux and
+//          update each run once per cell with every lane busy.
 // y-sweep  (Uin -> Uout): one thread per column; each warp marches down a
 //          segment of rows with a sliding window (W(r-2), W(r-1), the last
 //          right-biased state and the last face flux), held in registers or,
@@ -31,11 +30,9 @@
 namespace mhd {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int XS_TX = 28;       // interior cells per warp in the x-sweep (32 lanes - 4 halo)
-constexpr int XS_ROWS = 8;      // warps (rows) per x-sweep CTA
-// rows each x-sweep warp processes (with one-row prefetch) and the rows a
-// y-sweep warp takes are launch parameters (kDefaultXRpw, kDefaultYBand and, for
-// batches, kDefaultYSeg in mhd_common.cuh; the batch autotuner may pick others).
+// the x-sweep segment a warp marches and the rows a y-sweep warp takes are
+// launch parameters (kDefaultXRpw, kDefaultYBand and, for batches, kDefaultYSeg
+// in mhd_common.cuh; the batch autotuner may pick others).
 constexpr int YS_WARPS = 4;     // warps (row segments) per y-sweep CTA
 
 template <int N, typename T>
@@ -163,90 +160,188 @@ __device__ __forceinline__ bool update_cell(const R* U, const R* Fp, const R* Fm
     return false;
 }
 
-// ---------------------------------------------------------------------------
-// x-sweep
-// ---------------------------------------------------------------------------
-// One CTA of WARPS warps handles a 28-column tile over WARPS * rpw rows:
-// warp w takes rows  row_block*WARPS*rpw + w + k*WARPS  (k < rpw) and loads
-// the next row's cells before computing the current one, so the load latency
-// overlaps the arithmetic.
-template <class PH, int WARPS = XS_ROWS>
-__device__ __forceinline__ void x_tile(const DevGrid& in, const DevGrid& out, const StepParams& P, double dt,
-                                       double ch, int tile_x, int row_block, int rpw) {
-    using R = typename PH::Real;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int row0 = row_block * WARPS * rpw;
-    const int row_end = min(in.ny, row0 + WARPS * rpw);
-    int row = row0 + warp;
-    if (row >= row_end) return;  // whole warp: no block-level synchronisation follows
-    const int ng = in.ng, ib = ng, ie = ng + in.nx;
-    const int x = ib - 2 + tile_x * XS_TX + lane;
-    const bool xin = x < in.tnx();
-    const double g = P.gamma;
-    const double dtd = dt / P.dx;
-    const bool do_recon = lane >= 1 && lane <= 30 && x >= ib - 1 && x <= ie;
-    const bool do_face = lane >= 1 && lane <= 29 && x >= ib - 1 && x <= ie - 1;
-    const bool do_update = lane >= 2 && lane <= 29 && x >= ib && x < ie;
+// 16-byte shared-memory slots (four FP32 or two FP64 values): the sweeps keep
+// per-lane values in shared memory in these units, so a group of values moves
+// with one 128-bit access.
+template <typename R>
+struct Slot16;
+template <>
+struct Slot16<float> {
+    static constexpr int E = 4;
+    using V = float4;
+    __device__ static V pack(const float* v, int n, int g) {
+        const int k = 4 * g;
+        return make_float4(v[k], k + 1 < n ? v[k + 1] : 0.f, k + 2 < n ? v[k + 2] : 0.f, k + 3 < n ? v[k + 3] : 0.f);
+    }
+    __device__ static void unpack(V t, float* v, int n, int g) {
+        const int k = 4 * g;
+        v[k] = t.x;
+        if (k + 1 < n) v[k + 1] = t.y;
+        if (k + 2 < n) v[k + 2] = t.z;
+        if (k + 3 < n) v[k + 3] = t.w;
+    }
+};
+template <>
+struct Slot16<double> {
+    static constexpr int E = 2;
+    using V = double2;
+    __device__ static V pack(const double* v, int n, int g) {
+        const int k = 2 * g;
+        return make_double2(v[k], k + 1 < n ? v[k + 1] : 0.0);
+    }
+    __device__ static void unpack(V t, double* v, int n, int g) {
+        const int k = 2 * g;
+        v[k] = t.x;
+        if (k + 1 < n) v[k + 1] = t.y;
+    }
+};
 
-    R Unext[NV];
+// N values <-> ceil(N / E) slots of slot group g0 on, `stride` slots apart.
+template <typename R, int N, int STRIDE>
+__device__ __forceinline__ void slots_put(typename Slot16<R>::V* base, int g0, const R* v) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) Unext[k] = R(0);
-    Unext[RHO] = R(1);
-    if (xin) load_cell(in, x, ng + row, Unext);
-
-#pragma unroll 1
-    for (; row < row_end; row += WARPS) {
-        const int y = ng + row;
-        R U[NV], W[NV];
+    for (int g = 0; g < (N + Slot16<R>::E - 1) / Slot16<R>::E; ++g) base[(g0 + g) * STRIDE] = Slot16<R>::pack(v, N, g);
+}
+template <typename R, int N, int STRIDE>
+__device__ __forceinline__ void slots_get(const typename Slot16<R>::V* base, int g0, R* v) {
 #pragma unroll
-        for (int k = 0; k < NV; ++k) U[k] = Unext[k];
-        if (xin && row + WARPS < row_end) load_cell(in, x, y + WARPS, Unext);  // prefetch
-        PH::prim(U, g, W);
-
-        typename PH::Side L, Rt;
-#pragma unroll
-        for (int k = 0; k < PH::NS; ++k) { L.v[k] = R(0); Rt.v[k] = R(0); }
-        {
-            typename PH::Prim Wm, Wp, Wc;
-            shfl_up_n<PH::NW>(W, Wm.v, 1);
-            shfl_down_n<PH::NW>(W, Wp.v, 1);
-#pragma unroll
-            for (int k = 0; k < PH::NW; ++k) Wc.v[k] = W[k];
-            if (do_recon) PH::template recon<0>(Wm, Wc, Wp, dtd, ch, g, L, Rt);
-        }
-        typename PH::Side Ln;
-        shfl_down_n<PH::NS>(L.v, Ln.v, 1);
-        R F[NV];
-#pragma unroll
-        for (int k = 0; k < NV; ++k) F[k] = R(0);
-        if (do_face) PH::template face<0>(Rt, Ln, ch, g, F);
-        R Fm[NV];
-        shfl_up_n<NV>(F, Fm, 1);
-        if (do_update) {
-            R Un[NV];
-            const bool reverted = update_cell<R>(U, F, Fm, R(dtd), Un);
-            if (reverted && P.clock) atomicAdd(&P.clock->flux_fallbacks, 1u);
-            store_cell(out, x, y, Un);
-            if (near_edge(out, x, y)) scatter_ghosts<R>(out, x, y, Un, P.bc);
-        }
+    for (int g = 0; g < (N + Slot16<R>::E - 1) / Slot16<R>::E; ++g) {
+        const typename Slot16<R>::V t = base[(g0 + g) * STRIDE];
+        Slot16<R>::unpack(t, v, N, g);
     }
 }
 
+// ---------------------------------------------------------------------------
+// x-sweep
+// ---------------------------------------------------------------------------
+// A march along a row.  A warp takes one row segment of `len` interior cells
+// starting at interior column c0 and walks it in chunks of 32 consecutive
+// cells, lane l holding cell xs + q, q = 32 k + l (xs = ng + c0 - 2, two cells
+// before the segment).  At step q a lane computes the primitive state of cell
+// q, the reconstruction of cell q - 1, the face flux between cells q - 2 and
+// q - 1 and the update of cell q - 2 -- every cell and every face exactly once,
+// with all 32 lanes doing useful work except in the last, partial chunk of a
+// segment (segments are 32 m - 4 cells long, so a full segment fills its chunks
+// exactly).  The neighbour values a lane needs (W of cells q - 2 and q - 1, the
+// right-face state of cell q - 2, the flux of face (q - 3 | q - 2)) come from
+// three per-warp shared-memory rings of 64 entries, written one step earlier by
+// the neighbouring lane or, for lanes 0 and 1, by lanes 30 and 31 of the
+// previous chunk; a __syncwarp orders each write before the neighbouring lane's
+// read.  The cell updated at step q is reloaded from the input (L1-resident:
+// this warp loaded it two cells before).
+template <class PH>
+struct XRing {
+    using R = typename PH::Real;
+    static constexpr int E = Slot16<R>::E;
+    static constexpr int GW = (PH::NW + E - 1) / E;   // slot groups of a primitive state
+    static constexpr int GS = (PH::NS + E - 1) / E;   // of a face-side state
+    static constexpr int GF = (NV + E - 1) / E;       // of a face flux
+    static constexpr int kEntries = 64;
+    static constexpr int kGroups = GW + GS + GF;
+    static constexpr int kWarpBytes = kGroups * kEntries * 16;
+};
+
+template <typename R>
+__device__ __forceinline__ void load_cell_or_rest(const DevGrid& g, int x, int y, R* U) {
+    if (x < g.tnx()) {
+        load_cell(g, x, y, U);
+    } else {  // past the grid: a state at rest that only feeds lanes storing nothing
+#pragma unroll
+        for (int k = 0; k < NV; ++k) U[k] = R(0);
+        U[RHO] = R(1);
+        U[EN] = R(1);
+    }
+}
+
+template <class PH>
+__device__ __forceinline__ void x_segment(const DevGrid& in, const DevGrid& out, const StepParams& P, double dt,
+                                          double ch, int y, int c0, int len,
+                                          typename Slot16<typename PH::Real>::V* ring) {
+    using R = typename PH::Real;
+    using X = XRing<PH>;
+    constexpr int NE = X::kEntries;
+    const int lane = threadIdx.x & 31;
+    const int xs = in.ng + c0 - 2;        // storage column of step q = 0
+    const int nk = (len + 4 + 31) >> 5;   // chunks: steps q = 0 .. len + 3
+    const double g = P.gamma;
+    const double dtd = dt / P.dx;
+    unsigned reverts = 0;
+    R Unext[NV];
+    __syncwarp();  // a warp that marched a segment before may still be reading its ring
+    load_cell_or_rest(in, xs + lane, y, Unext);
+#pragma unroll 1
+    for (int k = 0; k < nk; ++k) {
+        const int q = 32 * k + lane;
+        const int x = xs + q;
+        typename PH::Prim Wm, Wc, Wp;
+        {
+            R U[NV];
+#pragma unroll
+            for (int f = 0; f < NV; ++f) U[f] = Unext[f];
+            if (k + 1 < nk) load_cell_or_rest(in, x + 32, y, Unext);  // prefetch the next chunk
+            PH::prim(U, g, Wp.v);
+        }
+        typename Slot16<R>::V* const e0 = ring + (q & 63);
+        typename Slot16<R>::V* const e1 = ring + ((q - 1) & 63);
+        typename Slot16<R>::V* const e2 = ring + ((q - 2) & 63);
+        slots_put<R, PH::NW, NE>(e0, 0, Wp.v);
+        __syncwarp();
+        slots_get<R, PH::NW, NE>(e2, 0, Wm.v);
+        slots_get<R, PH::NW, NE>(e1, 0, Wc.v);
+        typename PH::Side L, Rt;
+        PH::template recon<0>(Wm, Wc, Wp, dtd, ch, g, L, Rt);  // cell q - 1 (valid for q >= 2)
+        slots_put<R, PH::NS, NE>(e1, X::GW, Rt.v);
+        __syncwarp();
+        R F[NV];
+        {
+            typename PH::Side Rl;
+            slots_get<R, PH::NS, NE>(e2, X::GW, Rl.v);
+            PH::template face<0>(Rl, L, ch, g, F);  // face (q - 2 | q - 1) (valid for q >= 3)
+        }
+        slots_put<R, NV, NE>(e1, X::GW + X::GS, F);
+        __syncwarp();
+        const int cell = q - 4;  // segment cell updated at this step: storage column x - 2
+        if (cell >= 0 && cell < len) {
+            R Fm[NV], Uc[NV], Un[NV];
+            slots_get<R, NV, NE>(e2, X::GW + X::GS, Fm);  // face (q - 3 | q - 2)
+            load_cell(in, x - 2, y, Uc);
+            reverts += update_cell<R>(Uc, F, Fm, R(dtd), Un) ? 1u : 0u;
+            store_cell(out, x - 2, y, Un);
+            if (near_edge(out, x - 2, y)) scatter_ghosts<R>(out, x - 2, y, Un, P.bc);
+        }
+    }
+    if (reverts && P.clock) atomicAdd(&P.clock->flux_fallbacks, reverts);
+}
+
+// Interior cells per x-sweep segment of `chunks` 32-cell chunks.
+__host__ __device__ __forceinline__ int x_seg_len(int chunks) { return 32 * chunks - 4; }
+
 // CTA shape and register budget per policy: PH::kXWarps warps per CTA,
-// PH::kXBlocks CTAs per SM.
+// PH::kXBlocks CTAs per SM; each warp takes one (row, segment) task, segments
+// of x_seg_len(chunks) cells, consecutive tasks on adjacent rows.  The rings
+// live in dynamic shared memory: kXWarps * XRing<PH>::kWarpBytes.
 template <class PH>
 __global__ void __launch_bounds__(32 * PH::kXWarps, PH::kXBlocks)
-    sweep_x_kernel(DevGrid in, DevGrid out, StepParams P, int rpw) {
+    sweep_x_kernel(DevGrid in, DevGrid out, StepParams P, int chunks) {
     using R = typename PH::Real;
+    using V = typename Slot16<R>::V;
+    extern __shared__ __align__(16) unsigned char xs_smem[];
     double dt, ch, damp;
-    const bool first = (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0);
+    const bool first = (blockIdx.x == 0 && threadIdx.x == 0);
     if (!step_scalars(P, dt, ch, damp)) {
         if (first) clock_flag_skip(P);
         return;
     }
     if (first && P.clock) P.clock->maxbits[P.parity ^ 1] = 0ull;
-    if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
-    x_tile<PH, PH::kXWarps>(in, out, P, dt, ch, blockIdx.x, blockIdx.y, rpw);
+    if (P.any_dirichlet && !P.no_gather) gather_dirichlet_ghosts<R>(in, out, P.bc);
+    const int warp = threadIdx.x >> 5;
+    const int len = x_seg_len(chunks);
+    const int segs = (in.nx + len - 1) / len;
+    const long long task = (long long)blockIdx.x * PH::kXWarps + warp;
+    if (task >= (long long)segs * in.ny) return;  // whole warp: no block-level synchronisation follows
+    const int row = (int)(task % in.ny), c0 = (int)(task / in.ny) * len;
+    V* ring = reinterpret_cast<V*>(xs_smem + warp * XRing<PH>::kWarpBytes);
+    x_segment<PH>(in, out, P, dt, ch, in.ng + row, c0, min(len, in.nx - c0), ring);
 }
 
 // ---------------------------------------------------------------------------
@@ -317,15 +412,22 @@ __device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out,
 // The same march with its loop-carried values -- the two previous primitive
 // rows (a ring indexed by row parity), the last right-biased state and the
 // last face flux -- kept in per-lane shared-memory slots instead of registers.
-// Slot s of a lane is carry[s * 32 + lane]: a warp's access is one
-// conflict-free row and no other thread reads it, so no synchronisation is
-// needed.  Moving these 2*NW + NS + NV values out of the register file lets
-// the sweep run at the x-sweep's register budget (more resident warps) for a
-// few shared-memory loads and stores per cell; values and operation order are
-// those of y_segment, so results are identical.
+// Slot group g of a lane is carry[g * 32 + lane] (16 bytes: four FP32 or two
+// FP64 values move with one 128-bit access); a warp's access is one contiguous,
+// conflict-free row of 512 bytes and no other thread reads it, so no
+// synchronisation is needed.  Moving these 2*NW + NS + NV values out of the
+// register file lets the sweep run at the x-sweep's register budget (more
+// resident warps) for a few shared-memory loads and stores per cell; values and
+// operation order are those of y_segment, so results are identical.
 template <class PH>
 struct YCarry {
-    static constexpr int kSlots = 2 * PH::NW + PH::NS + NV;
+    using R = typename PH::Real;
+    static constexpr int E = Slot16<R>::E;
+    static constexpr int GW = (PH::NW + E - 1) / E;  // slot groups of one primitive row
+    static constexpr int GS = (PH::NS + E - 1) / E;  // of one side state
+    static constexpr int GF = (NV + E - 1) / E;      // of one face flux
+    static constexpr int kGroups = 2 * GW + GS + GF;
+    static constexpr int kSlots = kGroups * E;        // R values per lane (the shared array's unit)
 };
 
 template <class PH>
@@ -333,6 +435,8 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
                                                   double dt, double ch, double damp, int strip, int j0, int count,
                                                   double& vmax, unsigned& reverts, typename PH::Real* carry) {
     using R = typename PH::Real;
+    using C = YCarry<PH>;
+    using V = typename Slot16<R>::V;
     const int lane = threadIdx.x & 31;
     const int ng = in.ng, ib = ng, ie = ng + in.nx;
     const int x = strip * 32 + lane;
@@ -341,9 +445,9 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
     const double g = P.gamma;
     const double dtd = dt / P.dy;
     typename PH::SpeedAcc acc = PH::no_speed();
-    R* const wring = carry + lane;                    // W of row k: slots (k & 1) * NW + [0, NW)
-    R* const rslot = carry + 2 * PH::NW * 32 + lane;  // last right-biased state: NS slots
-    R* const fslot = rslot + PH::NS * 32;             // last face flux: NV slots
+    V* const lb = reinterpret_cast<V*>(carry) + lane;  // this lane's slot groups, 32 slots apart
+    constexpr int RS = 2 * C::GW;                      // last right-biased state
+    constexpr int FS = RS + C::GS;                     // last face flux
 
     if (active) {
         typename PH::Prim Wm, Wc, Wp;
@@ -353,11 +457,9 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
         load_cell(in, x, j0 - 2, U);
         load_cell(in, x, j0 - 1, Unext);
         PH::prim(U, g, Wp.v);
-#pragma unroll
-        for (int k = 0; k < PH::NW; ++k) wring[(((j0 - 2) & 1) * PH::NW + k) * 32] = Wp.v[k];
+        slots_put<R, PH::NW, 32>(lb, ((j0 - 2) & 1) * C::GW, Wp.v);
         PH::prim(Unext, g, Wp.v);
-#pragma unroll
-        for (int k = 0; k < PH::NW; ++k) wring[(((j0 - 1) & 1) * PH::NW + k) * 32] = Wp.v[k];
+        slots_put<R, PH::NW, 32>(lb, ((j0 - 1) & 1) * C::GW, Wp.v);
         load_cell(in, x, j0, Unext);
 #pragma unroll 1
         for (int r = j0; r <= j1 + 1; ++r) {
@@ -367,33 +469,28 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
             R Uc[NV];
             if (r >= j0 + 2) load_cell(in, x, r - 2, Uc);  // the row updated below
             PH::prim(U, g, Wp.v);
-            R* const wm = wring + (r & 1) * PH::NW * 32;        // row r - 2, overwritten by row r
-            R* const wc = wring + ((r - 1) & 1) * PH::NW * 32;  // row r - 1
-#pragma unroll
-            for (int k = 0; k < PH::NW; ++k) { Wm.v[k] = wm[k * 32]; Wc.v[k] = wc[k * 32]; }
-#pragma unroll
-            for (int k = 0; k < PH::NW; ++k) wm[k * 32] = Wp.v[k];
+            const int gm = (r & 1) * C::GW;          // row r - 2, overwritten by row r
+            const int gc = ((r - 1) & 1) * C::GW;    // row r - 1
+            slots_get<R, PH::NW, 32>(lb, gm, Wm.v);
+            slots_get<R, PH::NW, 32>(lb, gc, Wc.v);
+            slots_put<R, PH::NW, 32>(lb, gm, Wp.v);
             PH::template recon<1>(Wm, Wc, Wp, dtd, ch, g, L, Rt);  // cell r-1
             if (r >= j0 + 1) {
-#pragma unroll
-                for (int k = 0; k < PH::NS; ++k) Rprev.v[k] = rslot[k * 32];
+                slots_get<R, PH::NS, 32>(lb, RS, Rprev.v);
                 PH::template face<1>(Rprev, L, ch, g, F);  // face (r-2 | r-1)
                 if (r >= j0 + 2) {
                     const int yc = r - 2;
                     R Fprev[NV], Un[NV];
-#pragma unroll
-                    for (int k = 0; k < NV; ++k) Fprev[k] = fslot[k * 32];
+                    slots_get<R, NV, 32>(lb, FS, Fprev);
                     reverts += update_cell<R>(Uc, F, Fprev, R(dtd), Un) ? 1u : 0u;
                     if (near_edge(out, x, yc)) scatter_ghosts<R>(out, x, yc, Un, P.bc);
                     Un[PSI] = Un[PSI] * R(damp);
                     store_cell(out, x, yc, Un);
                     if (P.accumulate) PH::fold_speed(Un, g, ch, acc);
                 }
-#pragma unroll
-                for (int k = 0; k < NV; ++k) fslot[k * 32] = F[k];
+                slots_put<R, NV, 32>(lb, FS, F);
             }
-#pragma unroll
-            for (int k = 0; k < PH::NS; ++k) rslot[k * 32] = Rt.v[k];
+            slots_put<R, PH::NS, 32>(lb, RS, Rt.v);
         }
     }
     if (P.accumulate) {
@@ -461,18 +558,19 @@ __global__ void __launch_bounds__(32 * PH::kYWarps, PH::kYBlocks) sweep_y_kernel
         if (first) clock_flag_skip(P);
         return;
     }
-    if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
+    if (P.any_dirichlet && !P.no_gather) gather_dirichlet_ghosts<R>(in, out, P.bc);
     const int strips = y_strips(in);
     const int w = blockIdx.x * PH::kYWarps + threadIdx.y;
-    const int r0 = (w / strips) * per;
-    __shared__ R carry[PH::kYCarry ? PH::kYWarps * YCarry<PH>::kSlots * 32 : 1];
+    const int row_end = P.nrows > 0 ? P.row0 + P.nrows : in.ny;  // the launch's interior row window
+    const int r0 = P.row0 + (w / strips) * per;
+    __shared__ __align__(16) R carry[PH::kYCarry ? PH::kYWarps * YCarry<PH>::kSlots * 32 : 1];
     double vmax = 0.0;
     unsigned reverts = 0;
-    if (r0 < in.ny)
-        y_march<PH>(in, out, P, dt, ch, damp, w % strips, in.ng + r0, min(per, in.ny - r0), vmax, reverts,
+    if (r0 < row_end)
+        y_march<PH>(in, out, P, dt, ch, damp, w % strips, in.ng + r0, min(per, row_end - r0), vmax, reverts,
                     carry + threadIdx.y * YCarry<PH>::kSlots * 32);
     y_fold(P, vmax, reverts);
-    if (P.clock && first) clock_advance(P, dt, ch);
+    if (P.clock && first && !P.no_advance) clock_advance(P, dt, ch);
 }
 
 // Standalone CFL maximum over the interior (compute_dt, src/cpu/solver_cpu.cpp:283-303)

@@ -255,17 +255,18 @@ __global__ void __launch_bounds__(32 * YT_WARPS, PH::kYTBlocks)
         if (first) clock_flag_skip(P);
         return;
     }
-    if (P.any_dirichlet) gather_dirichlet_ghosts<R>(in, out, P.bc);
+    if (P.any_dirichlet && !P.no_gather) gather_dirichlet_ghosts<R>(in, out, P.bc);
     const int groups = (y_strips(in) + YT_WARPS - 1) / YT_WARPS;
     const int band = blockIdx.x / groups;
-    const int r0 = band * per;
+    const int row_end = P.nrows > 0 ? P.row0 + P.nrows : in.ny;  // the launch's interior row window
+    const int r0 = P.row0 + band * per;
     double vmax = 0.0;
     unsigned reverts = 0;
-    if (r0 < in.ny)  // uniform over the CTA
+    if (r0 < row_end)  // uniform over the CTA
         y_band_tma<PH>(&map, in, out, P, dt, ch, damp, (blockIdx.x % groups) * YT_COLS, in.ng + r0,
-                       min(per, in.ny - r0), yt_smem, vmax, reverts);
+                       min(per, row_end - r0), yt_smem, vmax, reverts);
     y_fold(P, vmax, reverts);
-    if (P.clock && first) clock_advance(P, dt, ch);
+    if (P.clock && first && !P.no_advance) clock_advance(P, dt, ch);
 }
 
 }  // namespace mhd

@@ -16,24 +16,68 @@ A side between two slabs is declared Dirichlet to the kernels: they then copy
 reads them, and no kernel reads a state's y-ghost rows otherwise.  The global
 y boundaries keep their own type; with periodic y the slabs form a ring.
 
+The step is device-resident: dt, c_h and the psi damping factor come from
+each slab workspace's device clock (mhd_clock_start / mhd_sweep_clocked, as in
+the single-grid graph loop mhd_run), the global CFL maximum is a max-reduce of
+the clock slots between steps (int64 view of the bit pattern), and nothing is
+read back to the host.  The y-sweep of each slab runs first over the interior
+rows that need no halo (rows 2 .. n-3 of n), concurrently with the halo
+exchange on a second stream, then over the two edge rows on each side once the
+exchange has landed; the last edge launch gathers the Dirichlet ghost cells and
+advances the clock.
+
 `SlabGrid` keeps all slabs on the current device (copies through
-mhd_grid_copy_rows) and is bit-identical to the single-grid step (every slab
-workspace steps with the global spacing, mhd_set_spacing).  `DistSlabRun`
-holds one slab per rank; its exchange, `exchange_rows`, sends the same rows
-with torch.distributed point-to-point operations (NCCL on GPUs, gloo on CPU).
+mhd_grid_copy_rows) and is bit-identical to the single-grid device loop
+(mhd_run; every slab workspace steps with the global spacing,
+mhd_set_spacing).  `DistSlabRun` holds one slab per rank; its exchange,
+`exchange_rows`, sends the same rows with torch.distributed point-to-point
+operations (NCCL on GPUs, gloo on CPU), and the CFL maximum is an
+all-reduce(max) of the clock slot.
 """
 from __future__ import annotations
 
 import ctypes as C
-import math
 
 import numpy as np
 
-from ._lib import check, load, mhd_grid
+from ._lib import check, load, mhd_grid, mhd_run_info
 from .solver import F64, BoundaryConfig, BoundaryType, GpuWorkspace, Grid2DGPU, init_gpu_workspace
 
 HALO = 2  # x-swept rows the y-sweep reads beyond a slab edge
 EXCHANGED = int(BoundaryType.Dirichlet)  # kernel boundary type of a side filled by the exchange
+SWEEP_NO_GATHER, SWEEP_NO_ADVANCE = 1, 2  # mhd_sweep_clocked flags
+
+
+def y_windows(n: int, exchanged: bool) -> tuple[list[tuple[int, int, int]], list[tuple[int, int, int]]]:
+    """(row0, nrows, flags) launches of a slab's y-sweep: those that read no halo
+    row (run while the exchange proceeds) and those after it.  Exactly one launch
+    gathers the Dirichlet ghost cells and advances the clock: the last one."""
+    if not exchanged or n <= 2 * HALO:
+        return [], [(0, 0, 0)]
+    quiet = SWEEP_NO_GATHER | SWEEP_NO_ADVANCE
+    return [(HALO, n - 2 * HALO, quiet)], [(0, HALO, quiet), (n - HALO, HALO, 0)]
+
+
+class _DevicePtr:
+    """__cuda_array_interface__ of a device pointer (shape, typestr)."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3}
+
+
+def clock_slot(ws, parity: int):
+    """int64 torch view of a workspace's device-clock slot (mhd_clock_slot)."""
+    import torch
+
+    p = C.c_void_p()
+    check(load().mhd_clock_slot(ws.ptr, int(parity), C.byref(p)), "mhd_clock_slot")
+    return torch.as_tensor(_DevicePtr(p.value, (1,), "<i8"), device="cuda")
+
+
+def _sweep(ws, src, dst, solver, bc_arr, direction, parity, row0=0, nrows=0, flags=0):
+    check(load().mhd_sweep_clocked(ws.ptr, C.byref(src.g), C.byref(dst.g), int(solver), bc_arr, direction, parity,
+                                   row0, nrows, flags), "mhd_sweep_clocked")
 
 
 def slab_rows(ny: int, parts: int) -> list[tuple[int, int]]:
@@ -142,43 +186,69 @@ class SlabGrid:
             if cr is not None:
                 ws.set_cr(cr)
 
-    def max_speed(self) -> float:
-        lib = load()
-        m = C.c_double()
-        best = 0.0
-        for ws, U in zip(self.ws, self.U):
-            check(lib.mhd_max_speed(ws.ptr, C.byref(U.g), C.byref(m)), "mhd_max_speed")
-            best = max(best, m.value)
-        return best
+    def start(self, cfl: float, t_end: float) -> None:
+        """Starts every slab's device clock on the current torch stream and sets
+        clock slot 0 to the global CFL maximum."""
+        import torch
 
-    def step(self, cfl: float, solver: int, bc, t_left: float = math.inf) -> float:
-        """One split step of the whole grid; returns dt (clamped to t_left)."""
+        self.stream = torch.cuda.current_stream()
+        self.xstream = torch.cuda.Stream()
         lib = load()
+        for ws, U in zip(self.ws, self.U):
+            ws.set_stream(self.stream.cuda_stream)
+            check(lib.mhd_clock_start(ws.ptr, C.byref(U.g), float(cfl), float(t_end)), "mhd_clock_start")
+        self.slots = [[clock_slot(ws, par) for ws in self.ws] for par in (0, 1)]
+        self._reduce(0)
+        self.k = 0
+
+    def _reduce(self, parity: int) -> None:
+        import torch
+
+        m = torch.max(torch.cat(self.slots[parity]))
+        for s in self.slots[parity]:
+            s.copy_(m.view(1))
+
+    def step(self, solver: int, bc) -> None:
+        """One split step of the whole grid, enqueued on the stream start() saw;
+        nothing is read back (info() reads the clock)."""
+        import torch
+
         b = BoundaryConfig.of(bc)
         periodic_y = int(b.bottom) == 0 and int(b.top) == 0
-        M = self.max_speed()
-        for ws in self.ws:
-            check(lib.mhd_set_ch(ws.ptr, M), "mhd_set_ch")
-        x0, x1, y0, y1 = self.extent
-        dx, dy = (x1 - x0) / self.nx, (y1 - y0) / self.ny
-        dt = cfl * (dy if dy < dx else dx) / M
-        dt = min(dt, t_left)
+        par = self.k & 1
         bcs = [(C.c_int * 4)(*slab_bc(b, p, self.parts)) for p in range(self.parts)]
+        exchanged = self.parts > 1
         for p in range(self.parts):
-            check(lib.mhd_sweep(self.ws[p].ptr, C.byref(self.U[p].g), C.byref(self.T[p].g), dt, int(solver), bcs[p], 0),
-                  "mhd_sweep(x)")
-        self.synchronize()
-        for s, sr, d, dr in halo_copies(self.rows, self.ng, periodic_y):
-            check(lib.mhd_grid_copy_rows(C.byref(self.T[s].g), sr, C.byref(self.T[d].g), dr, HALO, None),
-                  "mhd_grid_copy_rows")
-        check(lib.mhd_synchronize(self.ws[0].ptr), "mhd_synchronize")
-        for p in range(self.parts):
-            check(lib.mhd_sweep(self.ws[p].ptr, C.byref(self.T[p].g), C.byref(self.N[p].g), dt, int(solver), bcs[p], 1),
-                  "mhd_sweep(y)")
+            _sweep(self.ws[p], self.U[p], self.T[p], solver, bcs[p], 0, par)
+        copies = halo_copies(self.rows, self.ng, periodic_y)
+        if copies:
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+            self.xstream.wait_event(ev)
+            lib = load()
+            for s, sr, d, dr in copies:
+                check(lib.mhd_grid_copy_rows(C.byref(self.T[s].g), sr, C.byref(self.T[d].g), dr, HALO,
+                                             C.c_void_p(self.xstream.cuda_stream)), "mhd_grid_copy_rows")
+        plans = [y_windows(r1 - r0, exchanged) for r0, r1 in self.rows]
+        for p, (early, _) in enumerate(plans):  # rows that read no halo row, during the exchange
+            for row0, nrows, flags in early:
+                _sweep(self.ws[p], self.T[p], self.N[p], solver, bcs[p], 1, par, row0, nrows, flags)
+        if copies:
+            self.stream.wait_stream(self.xstream)
+        for p, (_, late) in enumerate(plans):
+            for row0, nrows, flags in late:
+                _sweep(self.ws[p], self.T[p], self.N[p], solver, bcs[p], 1, par, row0, nrows, flags)
+        self._reduce(par ^ 1)
         for p in range(self.parts):
             self.U[p].swap(self.N[p])
-        self.synchronize()
-        return dt
+        self.k += 1
+
+    def info(self) -> mhd_run_info:
+        """The clock (every slab's is the same): t, steps, dt, c_h, status."""
+        info = mhd_run_info()
+        for ws in self.ws:
+            check(load().mhd_clock_read(ws.ptr, C.byref(info)), "mhd_clock_read")
+        return info
 
     def synchronize(self) -> None:
         lib = load()
@@ -273,31 +343,55 @@ class DistSlabRun:
         for g in (self.U, self.T, self.N):
             g.upload(part)
 
-    def step(self, cfl: float, solver: int, bc) -> float:
+    def start(self, cfl: float, t_end: float) -> None:
+        """Starts this rank's device clock on the current torch stream; clock slot 0
+        becomes the global CFL maximum (all-reduce(max) across ranks)."""
         import torch
 
-        lib = load()
+        self.stream = torch.cuda.current_stream()
+        self.xstream = torch.cuda.Stream()
+        self.ws.set_stream(self.stream.cuda_stream)
+        check(load().mhd_clock_start(self.ws.ptr, C.byref(self.U.g), float(cfl), float(t_end)), "mhd_clock_start")
+        self.slots = [clock_slot(self.ws, par) for par in (0, 1)]
+        self.dist.all_reduce(self.slots[0], op=self.dist.ReduceOp.MAX)
+        self.k = 0
+
+    def step(self, solver: int, bc) -> None:
+        """One split step of this rank's slab, enqueued without any host round trip:
+        x-sweep; the halo exchange on a second stream while the y-sweep does the
+        rows that need no halo; the edge rows; all-reduce(max) of the next CFL
+        maximum.  Every rank calls it the same number of times."""
+        import torch
+
         b = BoundaryConfig.of(bc)
         periodic_y = int(b.bottom) == 0 and int(b.top) == 0
-        m = C.c_double()
-        check(lib.mhd_max_speed(self.ws.ptr, C.byref(self.U.g), C.byref(m)), "mhd_max_speed")
-        M = torch.tensor([m.value], dtype=torch.float64, device="cuda")
-        self.dist.all_reduce(M, op=self.dist.ReduceOp.MAX)
-        M = float(M.item())
-        check(lib.mhd_set_ch(self.ws.ptr, M), "mhd_set_ch")
-        dx, dy = self.dx, self.dy
-        dt = cfl * (dy if dy < dx else dx) / M
+        par = self.k & 1
         sbc = (C.c_int * 4)(*slab_bc(b, self.rank, self.world))
-        check(lib.mhd_sweep(self.ws.ptr, C.byref(self.U.g), C.byref(self.T.g), dt, int(solver), sbc, 0), "mhd_sweep(x)")
-        check(lib.mhd_synchronize(self.ws.ptr), "mhd_synchronize")
+        _sweep(self.ws, self.U, self.T, solver, sbc, 0, par)
         below, above = neighbours(self.rank, self.world, periodic_y)
         r0, r1 = self.rows[self.rank]
-        exchange_rows(grid_tensor(self.T.g), r1 - r0, self.ng, below, above, self.dist)
-        torch.cuda.synchronize()
-        check(lib.mhd_sweep(self.ws.ptr, C.byref(self.T.g), C.byref(self.N.g), dt, int(solver), sbc, 1), "mhd_sweep(y)")
+        exchanged = below is not None or above is not None
+        early, late = y_windows(r1 - r0, exchanged)
+        if exchanged:
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+            self.xstream.wait_event(ev)
+            with torch.cuda.stream(self.xstream):
+                exchange_rows(grid_tensor(self.T.g), r1 - r0, self.ng, below, above, self.dist)
+        for row0, nrows, flags in early:
+            _sweep(self.ws, self.T, self.N, solver, sbc, 1, par, row0, nrows, flags)
+        if exchanged:
+            self.stream.wait_stream(self.xstream)
+        for row0, nrows, flags in late:
+            _sweep(self.ws, self.T, self.N, solver, sbc, 1, par, row0, nrows, flags)
+        self.dist.all_reduce(self.slots[par ^ 1], op=self.dist.ReduceOp.MAX)
         self.U.swap(self.N)
-        check(lib.mhd_synchronize(self.ws.ptr), "mhd_synchronize")
-        return dt
+        self.k += 1
+
+    def info(self) -> mhd_run_info:
+        info = mhd_run_info()
+        check(load().mhd_clock_read(self.ws.ptr, C.byref(info)), "mhd_clock_read")
+        return info
 
     def destroy(self) -> None:
         self.ws.destroy()

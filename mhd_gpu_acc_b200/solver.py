@@ -24,13 +24,14 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import os
 import sys
 from dataclasses import dataclass, field
 
 import numpy as np
 
 from . import _lib
-from ._lib import check, load, mhd_grid, mhd_run_info
+from ._lib import check, load, mhd_grid, mhd_run_info, mhd_state_meta
 
 F64, F32 = 0, 1
 
@@ -188,6 +189,19 @@ class Grid2DGPU:
     def swap(self, other: "Grid2DGPU") -> None:
         check(load().mhd_grid_swap(C.byref(self.g), C.byref(other.g)), "mhd_grid_swap")
 
+    def save(self, path: str, t: float = 0.0, ch: float = 0.0, steps: int = 0) -> None:
+        """Binary state dump (mhd_state_save): the grid in its own precision, ghosts
+        included, with the time, c_h and step count a resumed run needs."""
+        meta = mhd_state_meta(float(t), float(ch), int(steps))
+        check(load().mhd_state_save(C.byref(self.g), os.fsencode(path), C.byref(meta)), "mhd_state_save")
+
+    def load_state(self, path: str) -> mhd_state_meta:
+        """Reads a mhd_state_save file into this grid (same shape and precision);
+        returns its (t, ch, steps)."""
+        meta = mhd_state_meta()
+        check(load().mhd_state_load(C.byref(self.g), os.fsencode(path), C.byref(meta)), "mhd_state_load")
+        return meta
+
     def release(self) -> None:
         if getattr(self, "g", None) is not None and self.g.data:
             load().mhd_grid_free(C.byref(self.g))
@@ -224,9 +238,9 @@ class GpuWorkspace:
         check(load().mhd_set_tma_wait_limit(self._req(), int(ns)), "mhd_set_tma_wait_limit")
 
     def set_sweep_shape(self, xrpw: int = 8, yband: int = 0, ystage: int = 0) -> None:
-        """Launch shape only: x-sweep rows per warp, y-sweep rows per warp band
-        (0: the precision's default), y-sweep rows staged by TMA (1) or loaded
-        per thread (0)."""
+        """Launch shape only: x-sweep work per warp (row segments of 128 * xrpw - 4
+        cells), y-sweep rows per warp band (0: the precision's default), y-sweep
+        rows staged by TMA (1) or loaded per thread (0)."""
         check(load().mhd_set_sweep_shape(self._req(), int(xrpw), int(yband), int(ystage)), "mhd_set_sweep_shape")
 
     @property

@@ -90,3 +90,4 @@ def device_loop(U0, nx, ny, ng, extent, gamma, cfl, solver, bc, limiter=0, max_s
     U.release()
     T.release()
     return out, info
+
