@@ -195,7 +195,6 @@ def test_mass_conservation_without_damping():
     (4, 256, 2, 1, 150, 1e-5),   # Orszag-Tang [0,1]^2, HLLD, van Leer
     (4, 256, 0, 1, 150, 1e-5),   # Orszag-Tang [0,1]^2, HLL (head/riemann.hpp:70-107), van Leer
     (4, 256, 3, 1, 150, 1e-5),   # Orszag-Tang [0,1]^2, FORCE (head/riemann.hpp:486-525), van Leer
-    (4, 256, 1, 0, 150, 1e-5),   # Orszag-Tang [0,1]^2, HLLC, minmod
     (5, 256, 1, 0, 120, 1e-5),   # Mach-10 shock-bubble, HLLC
     (5, 256, 2, 0, 120, 1e-5),   # Mach-10 shock-bubble, HLLD
     (6, 800, 2, 0, 0, 3e-5),     # Brio-Wu to t_end
