@@ -26,11 +26,16 @@ struct FastPolicy {
     // Default y band (rows one warp marches).  Measured at 4096^2 (HLLD, van
     // Leer): 24 rows 0.659 ms, 16 rows 0.664, 32 rows 0.667, 48 rows 0.698.
     static constexpr int kYBand = 24;
-    // x-sweep: 4 warps per CTA, 4 CTAs per SM (128 registers).  Measured at
-    // 4096^2 (HLLD, van Leer): 0.591 ms, against 0.612 ms for 8 x 2 and 0.651 ms
-    // for 4 x 5 (96 registers, spills).
+    // x-sweep (row march, segments of 1020 cells): 4 warps per CTA, 4 CTAs per
+    // SM (128 registers, 44 KB of rings per CTA).  Measured at 4096^2 (HLLD, van
+    // Leer): 0.549 ms; segments of 508 cells 0.545 ms, of 2044 cells 0.588 ms.
+    // (The lane-per-cell tile it replaced: 0.574 ms.)
     static constexpr int kXWarps = 4;
     static constexpr int kXBlocks = 4;
+    // Reloading the updated cell at the top of each x-march step needs 9 more
+    // registers across the solve: at 128 registers that spills, and measured
+    // 0.576 ms against 0.549 ms for the reload just before the update.
+    static constexpr bool kXEarlyReload = false;
     struct Prim { float v[NV]; };
     using Side = fast::Side;
 
@@ -58,8 +63,8 @@ struct FastPolicy {
     // The y-sweep's running CFL maximum: FP32, floored by c_h once at the end.
     using SpeedAcc = float;
     __device__ static SpeedAcc no_speed() { return -1.0f; }
-    __device__ static void fold_speed(const float* U, double g, double ch, SpeedAcc& acc) {
-        fast::fold_cell_speed(U, (float)g, (float)ch, acc);
+    __device__ static void fold_speed(const float* U, double g, double, SpeedAcc& acc) {
+        fast::fold_cell_speed(U, (float)g, acc);
     }
     __device__ static double speed_of(SpeedAcc acc, double ch) { return acc < 0.0f ? 0.0 : fmax((double)acc, ch); }
 };

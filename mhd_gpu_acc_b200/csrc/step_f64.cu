@@ -27,11 +27,14 @@ struct ExactPolicy {
     // Default y band.  Measured at 4096^2 (HLLD, van Leer): 32 rows 2.97 ms,
     // 24 rows 2.98, 48 rows 2.98, 16 rows 3.07.
     static constexpr int kYBand = 32;
-    // x-sweep: 4 warps per CTA, 3 CTAs per SM (168 registers, a few spilled).
-    // Measured at 4096^2 (HLLD, van Leer): 2.29 ms, against 2.65 ms for one CTA
-    // of 8 warps (240 registers) and 2.35 ms for 2 warps x 6.
+    // x-sweep (row march): 4 warps per CTA, 2 CTAs per SM (238 registers, no
+    // spills), the updated cell reloaded at the top of each step.  Measured at
+    // 4096^2 (HLLD, van Leer): 2.21 ms, against 2.27 ms reloading just before
+    // the update and 2.39 / 2.64 ms (early / late reload) at 3 CTAs per SM
+    // (168 registers, 128 / 360 bytes of spills).
     static constexpr int kXWarps = 4;
-    static constexpr int kXBlocks = 3;
+    static constexpr int kXBlocks = 2;
+    static constexpr bool kXEarlyReload = true;
     struct Prim { double v[NV]; };
     struct Side { double v[NV]; };
 

@@ -228,7 +228,9 @@ __device__ __forceinline__ void slots_get(const typename Slot16<R>::V* base, int
 // the neighbouring lane or, for lanes 0 and 1, by lanes 30 and 31 of the
 // previous chunk; a __syncwarp orders each write before the neighbouring lane's
 // read.  The cell updated at step q is reloaded from the input (L1-resident:
-// this warp loaded it two cells before).
+// this warp loaded it two cells before), at the top of the step when the policy
+// has the registers to hold it across the solve (kXEarlyReload), else just
+// before the update.
 template <class PH>
 struct XRing {
     using R = typename PH::Real;
@@ -281,6 +283,10 @@ __device__ __forceinline__ void x_segment(const DevGrid& in, const DevGrid& out,
             if (k + 1 < nk) load_cell_or_rest(in, x + 32, y, Unext);  // prefetch the next chunk
             PH::prim(U, g, Wp.v);
         }
+        const int cell = q - 4;  // segment cell updated at this step: storage column x - 2
+        const bool upd = cell >= 0 && cell < len;
+        R Uc[NV];
+        if (PH::kXEarlyReload && upd) load_cell(in, x - 2, y, Uc);  // its latency hides behind the solve
         typename Slot16<R>::V* const e0 = ring + (q & 63);
         typename Slot16<R>::V* const e1 = ring + ((q - 1) & 63);
         typename Slot16<R>::V* const e2 = ring + ((q - 2) & 63);
@@ -300,11 +306,10 @@ __device__ __forceinline__ void x_segment(const DevGrid& in, const DevGrid& out,
         }
         slots_put<R, NV, NE>(e1, X::GW + X::GS, F);
         __syncwarp();
-        const int cell = q - 4;  // segment cell updated at this step: storage column x - 2
-        if (cell >= 0 && cell < len) {
-            R Fm[NV], Uc[NV], Un[NV];
+        if (upd) {
+            R Fm[NV], Un[NV];
             slots_get<R, NV, NE>(e2, X::GW + X::GS, Fm);  // face (q - 3 | q - 2)
-            load_cell(in, x - 2, y, Uc);
+            if (!PH::kXEarlyReload) load_cell(in, x - 2, y, Uc);
             reverts += update_cell<R>(Uc, F, Fm, R(dtd), Un) ? 1u : 0u;
             store_cell(out, x - 2, y, Un);
             if (near_edge(out, x - 2, y)) scatter_ghosts<R>(out, x - 2, y, Un, P.bc);
