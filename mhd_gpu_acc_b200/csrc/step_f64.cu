@@ -22,6 +22,9 @@ struct ExactPolicy {
     // register window (255 registers, spills) and 3.06 ms for the shared-memory
     // window at 3 CTAs (168 registers, spills).
     static constexpr bool kYCarry = true;
+    // FP64 slots for the updated row would take the CTA's static shared memory
+    // past 48 KB: that row is reloaded from global memory.
+    static constexpr bool kYURing = false;
     static constexpr int kYBlocks = 2;  // y-sweep CTAs per SM the register budget is cut for
     static constexpr int kYTBlocks = 2; // the same for the TMA-staged y-sweep
     // Default y band.  Measured at 4096^2 (HLLD, van Leer): 32 rows 2.97 ms,

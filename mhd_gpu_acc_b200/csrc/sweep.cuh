@@ -423,7 +423,10 @@ __device__ __forceinline__ void y_segment(const DevGrid& in, const DevGrid& out,
 // synchronisation is needed.  Moving these 2*NW + NS + NV values out of the
 // register file lets the sweep run at the x-sweep's register budget (more
 // resident warps) for a few shared-memory loads and stores per cell; values and
-// operation order are those of y_segment, so results are identical.
+// operation order are those of y_segment, so results are identical.  When the
+// policy asks (kYURing), the conserved row r - 2 that step r updates also comes
+// from the slots (rows r - 2 and r share a slot pair by row parity) instead of
+// a second global load of that row.
 template <class PH>
 struct YCarry {
     using R = typename PH::Real;
@@ -431,7 +434,9 @@ struct YCarry {
     static constexpr int GW = (PH::NW + E - 1) / E;  // slot groups of one primitive row
     static constexpr int GS = (PH::NS + E - 1) / E;  // of one side state
     static constexpr int GF = (NV + E - 1) / E;      // of one face flux
-    static constexpr int kGroups = 2 * GW + GS + GF;
+    static constexpr bool kURing = PH::kYURing;       // conserved rows r - 2 / r in the slots too
+    static constexpr int GU = (NV + E - 1) / E;      // of one conserved row
+    static constexpr int kGroups = 2 * GW + GS + GF + (kURing ? 2 * GU : 0);
     static constexpr int kSlots = kGroups * E;        // R values per lane (the shared array's unit)
 };
 
@@ -453,6 +458,7 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
     V* const lb = reinterpret_cast<V*>(carry) + lane;  // this lane's slot groups, 32 slots apart
     constexpr int RS = 2 * C::GW;                      // last right-biased state
     constexpr int FS = RS + C::GS;                     // last face flux
+    constexpr int US = FS + C::GF;                     // conserved rows r - 2 / r (ring by row parity)
 
     if (active) {
         typename PH::Prim Wm, Wc, Wp;
@@ -465,6 +471,7 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
         slots_put<R, PH::NW, 32>(lb, ((j0 - 2) & 1) * C::GW, Wp.v);
         PH::prim(Unext, g, Wp.v);
         slots_put<R, PH::NW, 32>(lb, ((j0 - 1) & 1) * C::GW, Wp.v);
+        if constexpr (C::kURing) slots_put<R, NV, 32>(lb, US + ((j0 - 1) & 1) * C::GU, Unext);
         load_cell(in, x, j0, Unext);
 #pragma unroll 1
         for (int r = j0; r <= j1 + 1; ++r) {
@@ -472,7 +479,12 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
             for (int k = 0; k < NV; ++k) U[k] = Unext[k];
             if (r <= j1) load_cell(in, x, r + 1, Unext);  // prefetch the next row
             R Uc[NV];
-            if (r >= j0 + 2) load_cell(in, x, r - 2, Uc);  // the row updated below
+            if constexpr (C::kURing) {
+                if (r >= j0 + 2) slots_get<R, NV, 32>(lb, US + (r & 1) * C::GU, Uc);  // the row updated below
+                slots_put<R, NV, 32>(lb, US + (r & 1) * C::GU, U);
+            } else if (r >= j0 + 2) {
+                load_cell(in, x, r - 2, Uc);
+            }
             PH::prim(U, g, Wp.v);
             const int gm = (r & 1) * C::GW;          // row r - 2, overwritten by row r
             const int gc = ((r - 1) & 1) * C::GW;    // row r - 1
