@@ -106,6 +106,21 @@ __global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) batch_y_kernel(co
     }
 }
 
+// The x phase's dynamic shared memory opt-in (once per policy, before any
+// stream capture: mhd_batch_run makes a which = 0 call first).
+template <class PH>
+cudaError_t bx_setup() {
+    static const cudaError_t e = [] {
+        cudaError_t r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             bx_smem_bytes<PH>());
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+        return r;
+    }();
+    return e;
+}
+
 struct BatchLaunch {
     const BatchInst* inst;
     const int* first;
@@ -113,16 +128,9 @@ struct BatchLaunch {
     cudaStream_t st;
     template <class PH>
     cudaError_t run() const {
+        const cudaError_t attr = bx_setup<PH>();
+        if (attr != cudaSuccess || which == 0) return attr;  // which 0: the set-up alone
         if (which == 1) {
-            static const cudaError_t attr = [] {
-                cudaError_t r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     bx_smem_bytes<PH>());
-                if (r == cudaSuccess)
-                    r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                             (int)cudaSharedmemCarveoutMaxShared);
-                return r;
-            }();
-            if (attr != cudaSuccess) return attr;
             batch_x_kernel<PH><<<ctas, 32 * BX_WARPS, bx_smem_bytes<PH>(), st>>>(inst, first, n, parity, xrpw);
         }
         else batch_y_kernel<PH><<<ctas, dim3(32, YS_WARPS), 0, st>>>(inst, first + n + 1, n, parity, yseg);

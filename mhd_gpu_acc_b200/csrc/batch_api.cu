@@ -277,6 +277,7 @@ int mhd_batch_run(mhd_batch* b, int max_steps, mhd_run_info* info) {
             own = true;
         }
         cudaGraph_t gr = nullptr;
+        BCK(phase(b, 0, 0, b->tune, cap));  // kernel attribute set-up, outside the capture
         BCK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
         for (int p = 0; p < 2 && e == cudaSuccess; ++p) {
