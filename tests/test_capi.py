@@ -102,3 +102,31 @@ def test_batch_tune_candidates_exported():
     from mhd_gpu_acc_b200 import load
 
     assert load().mhd_batch_tune_candidates(7, None, 0) < 0
+
+
+def test_state_file_header_checks_need_no_gpu(tmp_path, lib):
+    """mhd_state_load rejects a file that is not a state file, or one written
+    for another shape or precision, from its 128-byte header alone -- before
+    any device copy (so this runs without a GPU; the grid's data pointer is a
+    host stand-in that must never be dereferenced)."""
+    import struct
+
+    from mhd_gpu_acc_b200._lib import mhd_state_meta
+
+    g = mhd_grid()
+    stand_in = C.create_string_buffer(16)
+    g.data = C.cast(stand_in, C.c_void_p)
+    g.nx, g.ny, g.ng, g.dtype = 8, 6, 2, 0
+    g.pitch, g.plane = 32, 32 * 10
+    g.x_min, g.x_max, g.y_min, g.y_max = 0.0, 1.0, 0.0, 1.0
+    bad = tmp_path / "bad.mhd"
+    bad.write_bytes(b"not a state file" * 10)
+    meta = mhd_state_meta()
+    assert lib.mhd_state_load(C.byref(g), str(bad).encode(), C.byref(meta)) == -1
+    assert b"not a state file" in lib.mhd_last_error()
+    other = tmp_path / "other.mhd"
+    header = b"MHDB200S" + struct.pack("<II3i", 1, 0, 9, 6, 2) + bytes(128 - 28)
+    other.write_bytes(header)
+    assert lib.mhd_state_load(C.byref(g), str(other).encode(), C.byref(meta)) == -1
+    assert b"differs" in lib.mhd_last_error()
+    assert lib.mhd_state_load(C.byref(g), str(tmp_path / "missing.mhd").encode(), None) == -1
