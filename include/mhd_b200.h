@@ -114,8 +114,8 @@ int mhd_set_cr(mhd_workspace* ws, double cr);
  * y-sweep warp marches down (0 = the precision's default: 24 rows for FP32,
  * 32 for FP64), and how the y-sweep gets its rows:
  * ystage 0 (default) = per-thread loads, 1 = TMA boxes staged in shared memory
- * (same results; on B200 at 4096^2 FP32 the staged sweep measured 0.81 ms
- * against 0.72 ms). */
+ * (same results; on B200 at 4096^2 FP32 the staged sweep measured 0.77 ms
+ * against 0.62 ms for per-thread loads). */
 int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage);
 /* Limit, in nanoseconds of the GPU's global timer, of each wait of the
  * TMA-staged y-sweep (ystage 1) for a box of rows to land; 0 restores the
