@@ -55,10 +55,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="ot", choices=["ot", "batch", "adjoint", "precision"],
+    ap.add_argument("--workload", default="ot", choices=["ot", "batch", "adjoint", "precision", "slabs"],
                     help="ot: Orszag-Tang n^2 (default line); batch: 256 uneven Orszag-Tang instances; "
                          "adjoint: gradient of the Orszag-Tang objective; precision: FP32-bulk vs FP64 "
-                         "relative L1 / Linf per field of every configuration, run to t_end")
+                         "relative L1 / Linf per field of every configuration, run to t_end; slabs: one "
+                         "Orszag-Tang n^2 grid split into y-slabs (--parts on one GPU, or one slab per rank)")
+    ap.add_argument("--parts", type=int, default=4, help="slabs workload on one GPU: number of y-slabs")
     ap.add_argument("--precision-max-n", type=int, default=2048,
                     help="largest Orszag-Tang side of the precision workload (512, 2048, 4096)")
     ap.add_argument("--precision-cases", default="",
@@ -743,6 +745,93 @@ def run_precision(a, world, rank, local):
     return 0
 
 
+def run_slabs(a, world, rank, local):
+    """One Orszag-Tang n^2 grid (FP32-bulk, HLLD + van Leer) split into y-slabs and
+    stepped without host round trips (mhd_gpu_acc_b200.slabs): on one GPU as
+    `--parts` slabs (halo copies on a second stream), under torchrun as one slab
+    per rank (NCCL halo exchange and all-reduce(max)); strong scaling of the one
+    grid.  The final state is checked against the single-grid device loop (one
+    GPU: bit for bit; ranks: the density sum)."""
+    import numpy as np
+    import torch
+
+    import mhd_gpu_acc_b200 as m
+    from mhd_gpu_acc_b200.slabs import DistSlabRun, SlabGrid
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n = a.n
+    cfg = m.get_n_case_config(m.CaseId.OrszagTangUnit, 1)
+    solver, limiter, bc = m.RiemannSolver.HLLD, m.Limiter.VANLEER, (0, 0, 0, 0)
+    U0 = m.initialise(m.CaseId.OrszagTangUnit, n, n, 2, cfg.extent)
+    if world == 1:
+        run = SlabGrid(n, n, 2, cfg.extent, a.parts, m.F32)
+        run.upload(U0)
+        run.configure(cfg.gamma, limiter)
+    else:
+        run = DistSlabRun(n, n, 2, cfg.extent, m.F32)
+        run.upload(U0)
+        m.set_gpu_physics_gamma(run.ws, cfg.gamma)
+        m.set_gpu_physics_ch(run.ws, 0.0)
+        run.ws.set_limiter(limiter)
+    run.start(cfg.cfl, cfg.t_end)
+    for _ in range(a.warmup):
+        run.step(solver, bc)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = m.launch_count()
+    e0.record(run.stream)
+    for _ in range(a.steps):
+        run.step(solver, bc)
+    e1.record(run.stream)
+    torch.cuda.synchronize()
+    launches = m.launch_count() - l0
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    info = run.info()
+    if world == 1:
+        got = run.download()
+        run.destroy()
+        U = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
+        T = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
+        U.upload(U0)
+        ws = m.GpuWorkspace()
+        m.init_gpu_workspace(ws, U)
+        m.set_gpu_physics_gamma(ws, cfg.gamma)
+        ws.set_limiter(limiter)
+        ws.run(U, T, cfg.cfl, cfg.t_end, a.warmup + a.steps, solver, bc)
+        want = U.download()
+        ws.destroy()
+        check = {"single_grid_bit_equal": bool(np.array_equal(got[:, 2:-2, :], want[:, 2:-2, :]))}
+    else:
+        part = float(run.U.download()[0, 2:-2, 2:-2].sum())
+        run.destroy()
+        check = {"rho_sum": sum_over_ranks(part, world)}
+    if rank == 0:
+        line = {
+            "metric": "Orszag-Tang cell-updates/s, one grid in y-slabs (FP32-bulk)", "unit": UNIT,
+            "value": n * n * a.steps / (ms / 1e3), "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (deterministic Orszag-Tang initial data)",
+            "config": {"workload": f"orszag_tang_unit_{n}x{n}_slabs", "slabs": a.parts if world == 1 else world,
+                       "exchange": "mhd_grid_copy_rows on a second stream" if world == 1 else "NCCL send/recv",
+                       "solver": "hlld", "limiter": "vanleer"},
+            "steps_done": info.steps, "gpu_launches": launches, "check": check,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     a = parse()
     world, rank, local = dist_setup()
@@ -754,6 +843,8 @@ def main():
         return run_adjoint(a, world, rank, local)
     if a.workload == "precision":
         return run_precision(a, world, rank, local)
+    if a.workload == "slabs":
+        return run_slabs(a, world, rank, local)
     return run_ours(a, world, rank, local)
 
 
