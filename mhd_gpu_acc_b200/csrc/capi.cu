@@ -551,14 +551,15 @@ int mhd_grid_copy_rows(const mhd_grid* src, int src_row, mhd_grid* dst, int dst_
     const int sty = src->ny + 2 * src->ng, dty = dst->ny + 2 * dst->ng;
     if (nrows < 0 || src_row < 0 || dst_row < 0 || src_row + nrows > sty || dst_row + nrows > dty)
         return fail(MHD_ERR_ARG, "mhd_grid_copy_rows: rows out of range");
+    if (nrows == 0) return MHD_OK;
     const size_t e = elem_bytes(src->dtype);
-    const size_t bytes = (size_t)nrows * (size_t)src->pitch * e;
+    const size_t bytes = (size_t)nrows * (size_t)src->pitch * e;  // the rows of one field are contiguous
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    for (int f = 0; f < MHD_NV; ++f) {
-        const char* s = static_cast<const char*>(src->data) + ((size_t)f * src->plane + (size_t)src_row * src->pitch) * e;
-        char* d = static_cast<char*>(dst->data) + ((size_t)f * dst->plane + (size_t)dst_row * dst->pitch) * e;
-        CK(cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToDevice, st));
-    }
+    // one strided copy: 9 blocks (one per field), a plane apart in each grid
+    const char* s = static_cast<const char*>(src->data) + (size_t)src_row * src->pitch * e;
+    char* d = static_cast<char*>(dst->data) + (size_t)dst_row * dst->pitch * e;
+    CK(cudaMemcpy2DAsync(d, (size_t)dst->plane * e, s, (size_t)src->plane * e, bytes, MHD_NV,
+                         cudaMemcpyDeviceToDevice, st));
     return MHD_OK;
 }
 

@@ -2,15 +2,15 @@
 grid (one slab per GPU), and the same decomposition on one device.
 
 A step of the split scheme needs, between its two sweeps, the two x-swept rows
-on each side of a slab boundary: the y-sweep of row j reads rows j-2 .. j+1.
+on each side of a slab boundary: the y-sweep of row j reads rows j-2 .. j+2.
 The x-sweep is row-local and the CFL maximum is a max over cells, so a step on
 P slabs is
-    M = max over slabs of mhd_max_speed       (all-reduce(max) across ranks)
-    ch = M; dt = cfl * min(dx, dy) / M         (identical on every slab)
-    x-sweep of every slab (mhd_sweep, dir 0)
-    halo exchange: each slab's two first / last interior rows of the x-swept
-                   state -> the neighbour's ghost rows (2 x 9 rows per side)
-    y-sweep of every slab (mhd_sweep, dir 1)
+    M = the global CFL maximum of U              (a max over the slabs' clocks)
+    ch = M; dt = cfl * min(dx, dy) / M           (identical on every slab)
+    x-sweep of every slab, U -> T
+    halo exchange: each slab's two first / last interior rows of T -> the
+                   neighbour's ghost rows of T (2 x 9 rows per side)
+    y-sweep of every slab, T -> U (two states per slab, as in mhd_run)
 A side between two slabs is declared Dirichlet to the kernels: they then copy
 (not compute) its ghost rows, which the exchange overwrites before the y-sweep
 reads them, and no kernel reads a state's y-ghost rows otherwise.  The global
@@ -26,8 +26,8 @@ exchange on a second stream, then over the two edge rows on each side once the
 exchange has landed; the last edge launch gathers the Dirichlet ghost cells and
 advances the clock.
 
-`SlabGrid` keeps all slabs on the current device (copies through
-mhd_grid_copy_rows) and is bit-identical to the single-grid device loop
+`SlabGrid` keeps all slabs on the current device (one strided copy per halo
+block through mhd_grid_copy_rows) and is bit-identical to the single-grid device loop
 (mhd_run; every slab workspace steps with the global spacing,
 mhd_set_spacing).  `DistSlabRun` holds one slab per rank; its exchange,
 `exchange_rows`, sends the same rows with torch.distributed point-to-point
@@ -146,13 +146,12 @@ class SlabGrid:
         self.extent = tuple(float(v) for v in extent)
         x0, x1, y0, y1 = self.extent
         self.rows = slab_rows(ny, parts)
-        self.U, self.T, self.N, self.ws = [], [], [], []
+        self.U, self.T, self.ws = [], [], []
         for r0, r1 in self.rows:
             e = (x0, x1) + slab_extent(y0, y1, ny, r0, r1)
             U = Grid2DGPU(nx, r1 - r0, ng, *e, dtype)
             self.U.append(U)
             self.T.append(Grid2DGPU(nx, r1 - r0, ng, *e, dtype))
-            self.N.append(Grid2DGPU(nx, r1 - r0, ng, *e, dtype))
             ws = GpuWorkspace()
             init_gpu_workspace(ws, U)
             check(load().mhd_set_spacing(ws.ptr, (x1 - x0) / nx, (y1 - y0) / ny), "mhd_set_spacing")
@@ -161,9 +160,9 @@ class SlabGrid:
     def upload(self, host: np.ndarray) -> None:
         """Global dense FP64 SoA (9, ny+2ng, nx+2ng) -> slabs (each with its ng ghost rows)."""
         ng = self.ng
-        for (r0, r1), U, T, N in zip(self.rows, self.U, self.T, self.N):
+        for (r0, r1), U, T in zip(self.rows, self.U, self.T):
             part = np.ascontiguousarray(host[:, r0:r1 + 2 * ng, :])
-            for g in (U, T, N):
+            for g in (U, T):
                 g.upload(part)
 
     def download(self) -> np.ndarray:
@@ -232,15 +231,13 @@ class SlabGrid:
         plans = [y_windows(r1 - r0, exchanged) for r0, r1 in self.rows]
         for p, (early, _) in enumerate(plans):  # rows that read no halo row, during the exchange
             for row0, nrows, flags in early:
-                _sweep(self.ws[p], self.T[p], self.N[p], solver, bcs[p], 1, par, row0, nrows, flags)
+                _sweep(self.ws[p], self.T[p], self.U[p], solver, bcs[p], 1, par, row0, nrows, flags)
         if copies:
             self.stream.wait_stream(self.xstream)
         for p, (_, late) in enumerate(plans):
             for row0, nrows, flags in late:
-                _sweep(self.ws[p], self.T[p], self.N[p], solver, bcs[p], 1, par, row0, nrows, flags)
+                _sweep(self.ws[p], self.T[p], self.U[p], solver, bcs[p], 1, par, row0, nrows, flags)
         self._reduce(par ^ 1)
-        for p in range(self.parts):
-            self.U[p].swap(self.N[p])
         self.k += 1
 
     def info(self) -> mhd_run_info:
@@ -330,7 +327,6 @@ class DistSlabRun:
         e = (x0, x1) + slab_extent(y0, y1, ny, r0, r1)
         self.U = Grid2DGPU(nx, r1 - r0, ng, *e, dtype)
         self.T = Grid2DGPU(nx, r1 - r0, ng, *e, dtype)
-        self.N = Grid2DGPU(nx, r1 - r0, ng, *e, dtype)
         self.ws = GpuWorkspace()
         init_gpu_workspace(self.ws, self.U)
         self.dx, self.dy = (x1 - x0) / nx, (y1 - y0) / ny
@@ -340,7 +336,7 @@ class DistSlabRun:
         """This rank's rows (with ghost rows) of the global dense FP64 SoA array."""
         r0, r1 = self.rows[self.rank]
         part = np.ascontiguousarray(host[:, r0:r1 + 2 * self.ng, :])
-        for g in (self.U, self.T, self.N):
+        for g in (self.U, self.T):
             g.upload(part)
 
     def start(self, cfl: float, t_end: float) -> None:
@@ -379,13 +375,12 @@ class DistSlabRun:
             with torch.cuda.stream(self.xstream):
                 exchange_rows(grid_tensor(self.T.g), r1 - r0, self.ng, below, above, self.dist)
         for row0, nrows, flags in early:
-            _sweep(self.ws, self.T, self.N, solver, sbc, 1, par, row0, nrows, flags)
+            _sweep(self.ws, self.T, self.U, solver, sbc, 1, par, row0, nrows, flags)
         if exchanged:
             self.stream.wait_stream(self.xstream)
         for row0, nrows, flags in late:
-            _sweep(self.ws, self.T, self.N, solver, sbc, 1, par, row0, nrows, flags)
+            _sweep(self.ws, self.T, self.U, solver, sbc, 1, par, row0, nrows, flags)
         self.dist.all_reduce(self.slots[par ^ 1], op=self.dist.ReduceOp.MAX)
-        self.U.swap(self.N)
         self.k += 1
 
     def info(self) -> mhd_run_info:
