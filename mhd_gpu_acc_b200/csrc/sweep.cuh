@@ -109,19 +109,31 @@ __device__ __forceinline__ bool near_edge(const DevGrid& g, int x, int y) {
 
 // Ghost cells of the sweep output that come from the INPUT grid: Dirichlet
 // sides (copy_ghost_cells) and corners whose rule passes through a Dirichlet
-// side.  Grid-stride over all ghost cells.
+// side.  Grid-stride over the ghost ring only -- the 2 ng full-width ghost rows,
+// then the 2 ng ghost columns of the interior rows -- so that a launch with few
+// threads (an edge-row window of the slab step) does not walk the interior.
 template <typename R>
 __device__ __forceinline__ void gather_dirichlet_ghosts(const DevGrid& in, const DevGrid& out, const int* bc) {
     const int ng = in.ng, ib = ng, ie = ng + in.nx, jb = ng, je = ng + in.ny;
-    const int tx = in.tnx(), ty = in.tny();
+    const int tx = in.tnx();
     const long long nthreads = (long long)gridDim.x * gridDim.y * blockDim.x * blockDim.y;
     const long long tid = ((long long)blockIdx.y * gridDim.x + blockIdx.x) * (blockDim.x * blockDim.y) +
                           threadIdx.y * blockDim.x + threadIdx.x;
-    const long long total = (long long)tx * ty;
+    const long long nrow = 2LL * ng * tx;  // ghost rows 0 .. ng-1 and je .. je+ng-1, full width
+    const long long total = nrow + 2LL * ng * in.ny;
     for (long long k = tid; k < total; k += nthreads) {
-        const int y = (int)(k / tx), x = (int)(k - (long long)y * tx);
+        int x, y;
+        if (k < nrow) {
+            const int r = (int)(k / tx);
+            x = (int)(k - (long long)r * tx);
+            y = r < ng ? r : in.ny + r;
+        } else {
+            const long long c = k - nrow;
+            const int r = (int)(c / (2 * ng)), q = (int)(c - (long long)r * 2 * ng);
+            y = jb + r;
+            x = q < ng ? q : in.nx + q;
+        }
         const bool xg = (x < ib || x >= ie), yg = (y < jb || y >= je);
-        if (!xg && !yg) continue;
         const int bcx = (x < ib) ? bc[0] : bc[1], bcy = (y < jb) ? bc[2] : bc[3];
         int srcx = x, srcy = y, fx = 0, fy = 0;
         if (xg && !yg) {
