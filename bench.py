@@ -368,56 +368,55 @@ def run_ours(a, world, rank, local):
     # the next uploads (the two copy directions run at once).  Two lanes
     # already keep both copy directions busy (three and four measured the
     # same), so the step is bound by the concurrent H2D + D2H rate.
-    e2e = None
-    if rank == 0 or True:
-        lanes = []
-        hin = torch.from_numpy(U0.astype(np.float32)).pin_memory()
-        a_in = hin.numpy()
-        for _ in range(a.e2e_lanes):
-            U = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
-            T = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
-            ws = m.GpuWorkspace()
-            m.init_gpu_workspace(ws, U)
-            m.set_gpu_physics_gamma(ws, cfg.gamma)
-            ws.set_limiter(limiter)
-            ws.set_sweep_shape(a.xrpw, a.yband, a.ystage)
-            s = torch.cuda.Stream()
-            ws.set_stream(s.cuda_stream)
-            hout = torch.empty_like(hin).pin_memory()
-            lanes.append((U, T, ws, s, hout.numpy(), hout))
+    # Every rank runs the loop (the time is the max over ranks).
+    lanes = []
+    hin = torch.from_numpy(U0.astype(np.float32)).pin_memory()
+    a_in = hin.numpy()
+    for _ in range(a.e2e_lanes):
+        U = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
+        T = m.Grid2DGPU(n, n, 2, *cfg.extent, m.F32)
+        ws = m.GpuWorkspace()
+        m.init_gpu_workspace(ws, U)
+        m.set_gpu_physics_gamma(ws, cfg.gamma)
+        ws.set_limiter(limiter)
+        ws.set_sweep_shape(a.xrpw, a.yband, a.ystage)
+        s = torch.cuda.Stream()
+        ws.set_stream(s.cuda_stream)
+        hout = torch.empty_like(hin).pin_memory()
+        lanes.append((U, T, ws, s, hout.numpy(), hout))
 
-        def e2e_step(k):
-            U, T, ws, _, a_out, _ = lanes[k % len(lanes)]
-            ws.upload_f32(U, a_in)
-            ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
-            ws.download_f32(U, a_out)
+    def e2e_step(k):
+        U, T, ws, _, a_out, _ = lanes[k % len(lanes)]
+        ws.upload_f32(U, a_in)
+        ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
+        ws.download_f32(U, a_out)
 
-        for k in range(4):  # warm-up
-            e2e_step(k)
-        torch.cuda.synchronize()
-        barrier(world)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _, _, _, s, _, _ in lanes:
-            s.wait_event(e0)
-        for k in range(a.e2e_steps):
-            e2e_step(k)
-        for _, _, _, s, _, _ in lanes:
-            ev = torch.cuda.Event()
-            ev.record(s)
-            stream.wait_event(ev)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = max_over_ranks(e0.elapsed_time(e1), world)
-        for _, _, ws, _, _, _ in lanes:
-            ws.destroy()
-        nbytes = int(hin.numel() * hin.element_size())
-        e2e = {"value": world * cells * a.e2e_steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
-               "d2h_bytes_per_step": nbytes, "steps": a.e2e_steps,
-               "what": "per step: H2D of the FP32 SoA state (ghosts included) from pinned memory "
-                       "(mhd_upload_f32), one FP32-bulk step (mhd_run), D2H of the state (mhd_download_f32); "
-                       f"{len(lanes)} workspaces on their own streams take steps in turn, so one step's download "
-                       "overlaps the next step's upload"}
+    for k in range(4):  # warm-up
+        e2e_step(k)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _, _, _, s, _, _ in lanes:
+        s.wait_event(e0)
+    for k in range(a.e2e_steps):
+        e2e_step(k)
+    for _, _, _, s, _, _ in lanes:
+        ev = torch.cuda.Event()
+        ev.record(s)
+        stream.wait_event(ev)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    for _, _, ws, _, _, _ in lanes:
+        ws.destroy()
+    nbytes = int(hin.numel() * hin.element_size())
+    e2e = {"value": world * cells * a.e2e_steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+           "d2h_bytes_per_step": nbytes, "steps": a.e2e_steps,
+           "what": "per step: H2D of the FP32 SoA state (ghosts included) from pinned memory "
+                   "(mhd_upload_f32), one FP32-bulk step (mhd_run), D2H of the state (mhd_download_f32); "
+                   f"{len(lanes)} workspaces on their own streams take steps in turn, so one step's download "
+                   "overlaps the next step's upload"}
 
     cpu = None
     if world == 1 and rank == 0 and not a.no_cpu_baseline:
@@ -439,7 +438,9 @@ def run_ours(a, world, rank, local):
                        "fp64 dt reduction)", "per_gpu": "one independent instance",
                        "l2": "state 604 MB (fp32) / 1.2 GB (fp64) > 126 MB L2; no flush",
                        "sweep_shape": {"xrpw": a.xrpw, "x_segment_cells": 128 * a.xrpw - 4,
+                                       "x_tail": "last quarter of each row in segments of a third",
                                        "yband": a.yband or "default (24 fp32, 32 fp64)",
+                                       "y_tail": "last eighth of the rows in bands of 1/2, last 1/32 of 1/4",
                                        "y_rows": "tma-staged" if a.ystage else "per-thread loads",
                                        "y_rows_note": "TMA-staged shared-memory boxes are a launch option "
                                                       "(--ystage 1); the per-thread loads measured faster for this "

@@ -57,26 +57,27 @@ cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
         if (e != cudaSuccess) return e;
     }
     if (which & 1) {
-        // xrpw sets the x-sweep work per warp: one row segment of 4 * xrpw chunks of 32 cells
-        const int chunks = 4 * xrpw;
-        const long long segs = (in.nx + x_seg_len(chunks) - 1) / x_seg_len(chunks);
-        const long long ctas = (segs * in.ny + PH::kXWarps - 1) / PH::kXWarps;
-        sweep_x_kernel<PH><<<(unsigned)ctas, 32 * PH::kXWarps, x_smem_bytes<PH>(), st>>>(in, tmp, P, chunks);
+        // xrpw sets the x-sweep work per warp: row segments of 4 * xrpw chunks of 32 cells (then shorter ones)
+        const SweepPlan pl = x_plan(in.nx, 4 * xrpw);
+        const long long ctas = (plan_tasks(pl, in.ny) + PH::kXWarps - 1) / PH::kXWarps;
+        sweep_x_kernel<PH><<<(unsigned)ctas, 32 * PH::kXWarps, x_smem_bytes<PH>(), st>>>(in, tmp, P, pl);
     }
     if (which & 2) {
         const int per = yband > 0 ? yband : PH::kYBand;
         const int rows = P.nrows > 0 ? P.nrows : tmp.ny - P.row0;  // the interior row window
-        const long long bands = (rows + per - 1) / per;
         alignas(64) CUtensorMap map;
         if (ystage == 1 && P.fault &&
             rows_tensor_map(&map, tmp, (int)sizeof(R), YT_COLS, YTShape<R>::ROWS)) {
+            // the TMA-staged y-sweep: one band height (its CTAs stage fixed boxes)
+            const long long bands = (rows + per - 1) / per;
             const long long groups = (y_strips(tmp) + YT_WARPS - 1) / YT_WARPS;
             sweep_y_tma_kernel<PH><<<(unsigned)(groups * bands), dim3(32, YT_WARPS), yt_smem_bytes<R>(), st>>>(
                 map, tmp, out, P, per);
         } else {
-            const long long warps = (long long)y_strips(tmp) * bands;
+            const SweepPlan pl = y_plan(rows, per);
+            const long long warps = plan_tasks(pl, y_strips(tmp));
             const unsigned grid = (unsigned)((warps + PH::kYWarps - 1) / PH::kYWarps);
-            sweep_y_kernel<PH><<<grid, dim3(32, PH::kYWarps), 0, st>>>(tmp, out, P, per);
+            sweep_y_kernel<PH><<<grid, dim3(32, PH::kYWarps), 0, st>>>(tmp, out, P, pl);
         }
     }
     return cudaGetLastError();

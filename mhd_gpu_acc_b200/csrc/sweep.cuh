@@ -333,13 +333,91 @@ __device__ __forceinline__ void x_segment(const DevGrid& in, const DevGrid& out,
 // Interior cells per x-sweep segment of `chunks` 32-cell chunks.
 __host__ __device__ __forceinline__ int x_seg_len(int chunks) { return 32 * chunks - 4; }
 
+// Guided task sizes.  A sweep launches several waves of tasks (4096^2 FP32:
+// ~7 waves of x segments, ~9 of y bands), and the tasks of the last wave end at
+// staggered times, which leaves SMs idle for up to one task's duration at the
+// end of the kernel.  So each sweep's work is cut into three phases of falling
+// task length, issued in order: long tasks for most of the grid, then shorter
+// ones, so that the long tasks' stragglers overlap short tasks and the kernel
+// ends on short tasks.  Phase p covers [lo[p], lo[p+1]) -- interior columns of
+// every row (x) or rows of every column strip (y) -- in n[p] tasks of len[p]
+// (the last task of phase 2 may be shorter); tasks run phase by phase, the
+// row (x) or strip (y) index fastest.
+struct SweepPlan {
+    int lo[4];
+    int len[3];
+    int n[3];
+};
+
+// Phase 0 ends at the last multiple of len0 at or below e0/64 of `total`,
+// phase 1 at the last multiple of len1 after that at or below e1/64 of it.
+__host__ __device__ inline SweepPlan guided_plan(int total, int len0, int len1, int len2, int e0, int e1) {
+    SweepPlan pl;
+    pl.len[0] = len0; pl.len[1] = len1; pl.len[2] = len2;
+    pl.lo[0] = 0;
+    pl.lo[1] = (int)(((long long)total * e0 / 64) / len0 * len0);
+    const int t1 = (int)((long long)total * e1 / 64);
+    pl.lo[2] = pl.lo[1] + (t1 > pl.lo[1] ? (t1 - pl.lo[1]) / len1 * len1 : 0);
+    pl.lo[3] = total;
+    pl.n[0] = pl.lo[1] / len0;
+    pl.n[1] = (pl.lo[2] - pl.lo[1]) / len1;
+    pl.n[2] = (total - pl.lo[2] + len2 - 1) / len2;
+    return pl;
+}
+
+__host__ __device__ inline long long plan_tasks(const SweepPlan& pl, int width) {
+    return (long long)(pl.n[0] + pl.n[1] + pl.n[2]) * width;
+}
+
+// Task k of a plan over `width` rows (x) or strips (y): its row / strip, first
+// column / row and length.  False past the last task.
+__device__ __forceinline__ bool plan_task(const SweepPlan& pl, long long k, int width, int& idx, int& start,
+                                          int& len) {
+    // selects rather than an indexed read, so the plan stays in the parameter bank
+    const long long n0 = (long long)pl.n[0] * width, n1 = (long long)pl.n[1] * width;
+    const long long n2 = (long long)pl.n[2] * width;
+    if (k >= n0 + n1 + n2) return false;
+    const bool p0 = k < n0, p1 = !p0 && k < n0 + n1;
+    k -= p0 ? 0 : (p1 ? n0 : n0 + n1);
+    const int lo = p0 ? pl.lo[0] : (p1 ? pl.lo[1] : pl.lo[2]);
+    const int hi = p0 ? pl.lo[1] : (p1 ? pl.lo[2] : pl.lo[3]);
+    const int l = p0 ? pl.len[0] : (p1 ? pl.len[1] : pl.len[2]);
+    idx = (int)(k % width);
+    start = lo + (int)(k / width) * l;
+    len = min(l, hi - start);
+    return true;
+}
+
+// Phase ends in 1/64 of the extent.  x: segments of the requested chunks up
+// to 3/4 of the row, then of 1/3 of them, the remainder (under one of those)
+// in segments of 1/9.  y: bands of the requested rows up to 7/8 of the rows,
+// then of 1/2 of them up to 31/32, then of 1/4 (a band carries a halo of four
+// rows, so the short phases stay small).  Measured on B200 at 4096^2 (HLLD,
+// van Leer; FP32 / FP64 ms): x 0.543 / 2.209 with one segment length, 0.513 /
+// 2.206 with these phases, 0.524 / 2.258 with a third phase of 92-cell
+// segments from 15/16 of the row; y 0.617 / 2.973 with one band height, 0.594 /
+// 2.919 with two phases (24 then 12 rows from 7/8), 0.582 / 2.891 with these,
+// 0.586 / 2.906 with the phases ending at 13/16 and 61/64.
+constexpr int kXPhase0End = 48, kXPhase1End = 64;
+constexpr int kYPhase0End = 56, kYPhase1End = 62;
+
+__host__ __device__ inline SweepPlan x_plan(int nx, int chunks) {
+    const int c1 = chunks / 3 > 1 ? chunks / 3 : 1, c2 = chunks / 9 > 1 ? chunks / 9 : 1;
+    return guided_plan(nx, x_seg_len(chunks), x_seg_len(c1), x_seg_len(c2), kXPhase0End, kXPhase1End);
+}
+
+__host__ __device__ inline SweepPlan y_plan(int rows, int per) {
+    const int p1 = per / 2 > 1 ? per / 2 : 1, p2 = per / 4 > 1 ? per / 4 : 1;
+    return guided_plan(rows, per, p1, p2, kYPhase0End, kYPhase1End);
+}
+
 // CTA shape and register budget per policy: PH::kXWarps warps per CTA,
-// PH::kXBlocks CTAs per SM; each warp takes one (row, segment) task, segments
-// of x_seg_len(chunks) cells, consecutive tasks on adjacent rows.  The rings
-// live in dynamic shared memory: kXWarps * XRing<PH>::kWarpBytes.
+// PH::kXBlocks CTAs per SM; each warp takes one (row, segment) task of the
+// plan (x_plan), consecutive tasks on adjacent rows.  The rings live in dynamic
+// shared memory: kXWarps * XRing<PH>::kWarpBytes.
 template <class PH>
 __global__ void __launch_bounds__(32 * PH::kXWarps, PH::kXBlocks)
-    sweep_x_kernel(DevGrid in, DevGrid out, StepParams P, int chunks) {
+    sweep_x_kernel(DevGrid in, DevGrid out, StepParams P, SweepPlan pl) {
     using R = typename PH::Real;
     using V = typename Slot16<R>::V;
     extern __shared__ __align__(16) unsigned char xs_smem[];
@@ -352,13 +430,11 @@ __global__ void __launch_bounds__(32 * PH::kXWarps, PH::kXBlocks)
     if (first && P.clock) P.clock->maxbits[P.parity ^ 1] = 0ull;
     if (P.any_dirichlet && !P.no_gather) gather_dirichlet_ghosts<R>(in, out, P.bc);
     const int warp = threadIdx.x >> 5;
-    const int len = x_seg_len(chunks);
-    const int segs = (in.nx + len - 1) / len;
     const long long task = (long long)blockIdx.x * PH::kXWarps + warp;
-    if (task >= (long long)segs * in.ny) return;  // whole warp: no block-level synchronisation follows
-    const int row = (int)(task % in.ny), c0 = (int)(task / in.ny) * len;
+    int row, c0, len;
+    if (!plan_task(pl, task, in.ny, row, c0, len)) return;  // whole warp: no block-level synchronisation follows
     V* ring = reinterpret_cast<V*>(xs_smem + warp * XRing<PH>::kWarpBytes);
-    x_segment<PH>(in, out, P, dt, ch, in.ng + row, c0, min(len, in.nx - c0), ring);
+    x_segment<PH>(in, out, P, dt, ch, in.ng + row, c0, len, ring);
 }
 
 // ---------------------------------------------------------------------------
@@ -566,20 +642,20 @@ __device__ __forceinline__ void clock_advance(const StepParams& P, double dt, do
     c->last_ch = ch;
 }
 
-// The y-sweep's work is `strips` column strips, each cut into row bands of
-// `per` rows (the policy's kYBand by default).  Warp w takes strip w % strips,
-// band w / strips: the warps of a CTA sit side by side on one band and
-// consecutive CTAs walk across the width first, so the resident CTAs cover a
-// narrow window of full-width rows that moves down the grid.  Measured on B200
-// (4096^2, FP32, register window): 32-row bands 0.72 ms, 64 rows 0.78 ms, 128
-// rows 0.96 ms, and one wave of ~300-row bands 1.31 ms -- short bands in a
-// moving window keep the segment
-// halos and the pages in use shared.
+// The y-sweep's work is `strips` column strips, each cut into row bands (the
+// policy's kYBand rows by default, shorter bands at the end: y_plan).  Warp w
+// takes task w of the plan, strip-fastest: the warps of a CTA sit side by side
+// on one band and consecutive CTAs walk across the width first, so the resident
+// CTAs cover a narrow window of full-width rows that moves down the grid.
+// Measured on B200 (4096^2, FP32, register window, one band height): 32-row
+// bands 0.72 ms, 64 rows 0.78 ms, 128 rows 0.96 ms, and one wave of ~300-row
+// bands 1.31 ms -- short bands in a moving window keep the segment halos and
+// the pages in use shared.
 __host__ __device__ __forceinline__ int y_strips(const DevGrid& g) { return (g.ng + g.nx + 31) / 32; }
 
 template <class PH>
 __global__ void __launch_bounds__(32 * PH::kYWarps, PH::kYBlocks) sweep_y_kernel(DevGrid in, DevGrid out,
-                                                                            StepParams P, int per) {
+                                                                            StepParams P, SweepPlan pl) {
     using R = typename PH::Real;
     double dt, ch, damp;
     const bool first = (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0);
@@ -588,15 +664,13 @@ __global__ void __launch_bounds__(32 * PH::kYWarps, PH::kYBlocks) sweep_y_kernel
         return;
     }
     if (P.any_dirichlet && !P.no_gather) gather_dirichlet_ghosts<R>(in, out, P.bc);
-    const int strips = y_strips(in);
     const int w = blockIdx.x * PH::kYWarps + threadIdx.y;
-    const int row_end = P.nrows > 0 ? P.row0 + P.nrows : in.ny;  // the launch's interior row window
-    const int r0 = P.row0 + (w / strips) * per;
+    int strip, r0, count;  // r0: first row of the band within the launch's interior row window (y_plan)
     __shared__ __align__(16) R carry[PH::kYCarry ? PH::kYWarps * YCarry<PH>::kSlots * 32 : 1];
     double vmax = 0.0;
     unsigned reverts = 0;
-    if (r0 < row_end)
-        y_march<PH>(in, out, P, dt, ch, damp, w % strips, in.ng + r0, min(per, row_end - r0), vmax, reverts,
+    if (plan_task(pl, w, y_strips(in), strip, r0, count))
+        y_march<PH>(in, out, P, dt, ch, damp, strip, in.ng + P.row0 + r0, count, vmax, reverts,
                     carry + threadIdx.y * YCarry<PH>::kSlots * 32);
     y_fold(P, vmax, reverts);
     if (P.clock && first && !P.no_advance) clock_advance(P, dt, ch);
