@@ -67,8 +67,8 @@ def parse():
                     help="comma-separated substrings: run only the precision cases whose names contain one")
     ap.add_argument("--seed", type=int, default=0, help="batch workload seed")
     ap.add_argument("--instances", type=int, default=256)
-    ap.add_argument("--xrpw", type=int, default=8,
-                    help="x-sweep work per warp: one row segment of 128 * xrpw - 4 cells")
+    ap.add_argument("--xrpw", type=int, default=0,
+                    help="x-sweep work per warp: row segments of 128 * xrpw - 4 cells (0: 8 for FP32, 16 for FP64)")
     ap.add_argument("--yband", type=int, default=0,
                     help="y-sweep rows per warp band (0: the precision's default, 24 FP32 / 32 FP64)")
     ap.add_argument("--ystage", type=int, default=0, choices=[0, 1],
@@ -437,9 +437,10 @@ def run_ours(a, world, rank, local):
                        "solver": "hlld", "limiter": "vanleer", "precision": "fp32-bulk (fp64 low-beta pressure, "
                        "fp64 dt reduction)", "per_gpu": "one independent instance",
                        "l2": "state 604 MB (fp32) / 1.2 GB (fp64) > 126 MB L2; no flush",
-                       "sweep_shape": {"xrpw": a.xrpw, "x_segment_cells": 128 * a.xrpw - 4,
+                       "sweep_shape": {"xrpw": a.xrpw or "default (8 fp32, 16 fp64)",
+                                       "x_segment_cells": 128 * (a.xrpw or 8) - 4,
                                        "x_tail": "last quarter of each row in segments of a third",
-                                       "yband": a.yband or "default (24 fp32, 32 fp64)",
+                                       "yband": a.yband or "default (28 fp32, 32 fp64)",
                                        "y_tail": "last eighth of the rows in bands of 1/2, last 1/32 of 1/4",
                                        "y_rows": "tma-staged" if a.ystage else "per-thread loads",
                                        "y_rows_note": "TMA-staged shared-memory boxes are a launch option "

@@ -109,15 +109,15 @@ int mhd_set_limiter(mhd_workspace* ws, int limiter);
 /* GLM damping ratio c_r = c_p^2 / c_h (default 0.18, head/physics.hpp:39). */
 int mhd_set_cr(mhd_workspace* ws, double cr);
 /* Launch shape of the sweeps (no reference counterpart; results do not depend
- * on it): the x-sweep work per warp, xrpw (default 8; one warp marches a row
- * segment of 128 * xrpw - 4 cells, the last quarter of each row in segments of
- * a third of that), the height of the row band one y-sweep warp marches down
- * (0 = the precision's default: 24 rows for FP32, 32 for FP64; the last eighth
- * of the rows in bands of a half and a quarter of that), and how the y-sweep
- * gets its rows: ystage 0 (default) = per-thread loads, 1 = TMA boxes staged in
- * shared memory, one band height (same results; on B200 at 4096^2 FP32 the
- * staged sweep measured 0.77 ms against 0.62 ms for per-thread loads with one
- * band height). */
+ * on it): the x-sweep work per warp, xrpw (0 = the precision's default: 8 for
+ * FP32, 16 for FP64; one warp marches a row segment of 128 * xrpw - 4 cells,
+ * the last quarter of each row in segments of a third of that), the height of
+ * the row band one y-sweep warp marches down (0 = the precision's default: 28
+ * rows for FP32, 32 for FP64; the last eighth of the rows in bands of a half
+ * and a quarter of that), and how the y-sweep gets its rows: ystage 0
+ * (default) = per-thread loads, 1 = TMA boxes staged in shared memory, one band
+ * height (same results; on B200 at 4096^2 FP32 the staged sweep measured
+ * 0.77 ms against 0.62 ms for per-thread loads with one band height). */
 int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage);
 /* Limit, in nanoseconds of the GPU's global timer, of each wait of the
  * TMA-staged y-sweep (ystage 1) for a box of rows to land; 0 restores the

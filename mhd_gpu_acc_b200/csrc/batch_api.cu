@@ -58,7 +58,7 @@ struct mhd_batch {
     mhd::DevClock* d_clock = nullptr;
     unsigned long long* d_max = nullptr;
     cudaStream_t stream = nullptr;
-    mhd_batch_tuning tune{mhd::kDefaultXRpw, mhd::kDefaultYSeg, 0, 0};
+    mhd_batch_tuning tune{mhd::kDefaultBatchXRpw, mhd::kDefaultYSeg, 0, 0};
     cudaGraphExec_t graph = nullptr;
     mhd_batch_tuning graph_tune{};
     long long cells = 0;

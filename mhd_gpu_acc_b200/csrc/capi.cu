@@ -436,8 +436,8 @@ int mhd_set_cr(mhd_workspace* ws, double cr) {
 
 int mhd_set_sweep_shape(mhd_workspace* ws, int xrpw, int yband, int ystage) {
     if (!ws) return fail(MHD_ERR_STATE, "mhd_set_sweep_shape: null workspace");
-    if (xrpw < 1 || xrpw > 64 || yband < 0 || yband > 65536 || ystage < 0 || ystage > 1)
-        return fail(MHD_ERR_ARG, "mhd_set_sweep_shape: need 1 <= xrpw <= 64, 0 <= yband <= 65536, ystage 0 or 1");
+    if (xrpw < 0 || xrpw > 64 || yband < 0 || yband > 65536 || ystage < 0 || ystage > 1)
+        return fail(MHD_ERR_ARG, "mhd_set_sweep_shape: need 0 <= xrpw <= 64, 0 <= yband <= 65536, ystage 0 or 1");
     ws->xrpw = xrpw;
     ws->yseg = yband;
     ws->ystage = ystage;

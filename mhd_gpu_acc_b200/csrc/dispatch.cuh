@@ -57,8 +57,9 @@ cudaError_t launch_policy(const DevGrid& in, const DevGrid& tmp, const DevGrid& 
         if (e != cudaSuccess) return e;
     }
     if (which & 1) {
-        // xrpw sets the x-sweep work per warp: row segments of 4 * xrpw chunks of 32 cells (then shorter ones)
-        const SweepPlan pl = x_plan(in.nx, 4 * xrpw);
+        // xrpw sets the x-sweep work per warp: row segments of 4 * xrpw chunks of 32 cells (then shorter
+        // ones); 0 = the policy's kXRpw
+        const SweepPlan pl = x_plan(in.nx, 4 * (xrpw > 0 ? xrpw : PH::kXRpw));
         const long long ctas = (plan_tasks(pl, in.ny) + PH::kXWarps - 1) / PH::kXWarps;
         sweep_x_kernel<PH><<<(unsigned)ctas, 32 * PH::kXWarps, x_smem_bytes<PH>(), st>>>(in, tmp, P, pl);
     }

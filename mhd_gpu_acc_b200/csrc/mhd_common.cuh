@@ -50,7 +50,8 @@ MHD_HD_RULE bool star_degenerate(float d, float rho, float un, float S, float SM
     const float m = fabsf(S) + fabsf(un) + fabsf(SM);
     return fabsf(d) <= kStarDegenRel * (rho * m * m + Bn * Bn);
 }
-constexpr int kDefaultXRpw = 8;  // x-sweep rows per warp
+constexpr int kDefaultXRpw = 0;  // x-sweep work per warp: 0 = the policy's kXRpw
+constexpr int kDefaultBatchXRpw = 8;  // batched x-sweep work per warp before tuning
 constexpr int kDefaultYSeg = 64; // batched y-sweep rows per warp segment
 constexpr int kDefaultYBand = 0;  // single-grid y-sweep rows per warp band: 0 = the policy's kYBand
 

@@ -569,5 +569,30 @@ __device__ __forceinline__ void fold_cell_speed(const float* U, float g, float& 
     acc = fmaxf(acc, fmaxf(fmaxf(a, b), 0.0f));
 }
 
+// fold_cell_speed for a reduction whose result is floored by c_h (speed_of),
+// as every y-sweep's is: a cell whose speed provably stays under the floor
+// cannot change the result, so its fast speeds are not computed.  The test is
+// an upper bound from the conserved state, max(|u|, |v|) + sqrt(a^2 + b^2) >=
+// max(|u| + c_fx, |v| + c_fy) (c_f^2 = (s + sqrt(s^2 - 4 a^2 b_n^2)) / 2 <= s =
+// a^2 + b^2), with a relative margin of 1e-5 over the rounding of both forms.
+// Only physical cells whose internal energy is above 1/40 of E are skipped, so
+// that c2p would take its FP32 branch and count the cell too (a skipped cell
+// is counted: acc >= 0); the others, and any non-finite cell, take the exact
+// path.  Measured on B200 (Orszag-Tang 4096^2, HLLD, van Leer): y-sweep
+// 0.582 -> 0.567 ms (bit-identical results).
+__device__ __forceinline__ void fold_cell_speed_floored(const float* U, float g, float floor_f, float& acc) {
+    const float r = U[RHO];
+    const float ir = 1.0f / r;
+    const float m2 = U[MX] * U[MX] + U[MY] * U[MY] + U[MZ] * U[MZ];
+    const float B2 = U[BX] * U[BX] + U[BY] * U[BY] + U[BZ] * U[BZ];
+    const float eint = U[EN] - 0.5f * (m2 * ir + B2);
+    const float bound = fmaxf(fabsf(U[MX]), fabsf(U[MY])) * ir + sqrtf((g * (g - 1.0f) * eint + B2) * ir);
+    if (r > 0.0f && eint > 0.025f * fabsf(U[EN]) && bound * 1.00001f < floor_f) {
+        acc = fmaxf(acc, 0.0f);
+        return;
+    }
+    fold_cell_speed(U, g, acc);
+}
+
 }  // namespace fast
 }  // namespace mhd

@@ -26,15 +26,21 @@ struct FastPolicy {
     static constexpr bool kYURing = true;
     static constexpr int kYBlocks = 4;  // y-sweep CTAs per SM the register budget is cut for
     static constexpr int kYTBlocks = 3; // the same for the TMA-staged y-sweep
-    // Default y band (rows one warp marches).  Measured at 4096^2 (HLLD, van
-    // Leer): 24 rows 0.659 ms, 16 rows 0.664, 32 rows 0.667, 48 rows 0.698.
-    static constexpr int kYBand = 24;
+    // Default y band (rows one warp marches; shorter bands at the end of the
+    // launch, y_plan).  Measured at 4096^2 (HLLD, van Leer) with the guided
+    // phases: 28 rows 0.566 ms, 24 rows 0.567, 32 rows 0.586 (before the CFL
+    // fold skip), 20 rows 0.594 (the same); with one band height: 24 rows
+    // 0.659 ms, 16 rows 0.664, 32 rows 0.667, 48 rows 0.698.
+    static constexpr int kYBand = 28;
     // x-sweep (row march, segments of 1020 cells): 4 warps per CTA, 4 CTAs per
     // SM (128 registers, 44 KB of rings per CTA).  Measured at 4096^2 (HLLD, van
     // Leer): 0.549 ms; segments of 508 cells 0.545 ms, of 2044 cells 0.588 ms.
     // (The lane-per-cell tile it replaced: 0.574 ms.)
     static constexpr int kXWarps = 4;
     static constexpr int kXBlocks = 4;
+    // Default x work per warp: segments of 1020 cells (the last quarter of a
+    // row in 316-cell ones); 2044-cell segments measured 0.520 ms, 508-cell 0.551.
+    static constexpr int kXRpw = 8;
     // Reloading the updated cell at the top of each x-march step needs 9 more
     // registers across the solve: at 128 registers that spills, and measured
     // 0.576 ms against 0.549 ms for the reload just before the update.
@@ -66,8 +72,8 @@ struct FastPolicy {
     // The y-sweep's running CFL maximum: FP32, floored by c_h once at the end.
     using SpeedAcc = float;
     __device__ static SpeedAcc no_speed() { return -1.0f; }
-    __device__ static void fold_speed(const float* U, double g, double, SpeedAcc& acc) {
-        fast::fold_cell_speed(U, (float)g, acc);
+    __device__ static void fold_speed(const float* U, double g, double ch, SpeedAcc& acc) {
+        fast::fold_cell_speed_floored(U, (float)g, (float)ch, acc);
     }
     __device__ static double speed_of(SpeedAcc acc, double ch) { return acc < 0.0f ? 0.0 : fmax((double)acc, ch); }
 };

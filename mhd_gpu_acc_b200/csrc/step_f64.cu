@@ -38,6 +38,10 @@ struct ExactPolicy {
     static constexpr int kXWarps = 4;
     static constexpr int kXBlocks = 2;
     static constexpr bool kXEarlyReload = true;
+    // Default x work per warp: segments of 2044 cells (the last quarter of a
+    // row in 668-cell ones).  Measured at 4096^2: 2.175 ms, against 2.210 ms
+    // for 1020-cell segments.
+    static constexpr int kXRpw = 16;
     struct Prim { double v[NV]; };
     struct Side { double v[NV]; };
 

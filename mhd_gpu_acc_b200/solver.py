@@ -237,10 +237,10 @@ class GpuWorkspace:
         """Limit (ns) of each wait for a TMA-staged y-sweep box; 0 = the 2 s default."""
         check(load().mhd_set_tma_wait_limit(self._req(), int(ns)), "mhd_set_tma_wait_limit")
 
-    def set_sweep_shape(self, xrpw: int = 8, yband: int = 0, ystage: int = 0) -> None:
+    def set_sweep_shape(self, xrpw: int = 0, yband: int = 0, ystage: int = 0) -> None:
         """Launch shape only: x-sweep work per warp (row segments of 128 * xrpw - 4
-        cells), y-sweep rows per warp band (0: the precision's default), y-sweep
-        rows staged by TMA (1) or loaded per thread (0)."""
+        cells; 0: the precision's default), y-sweep rows per warp band (0: the
+        precision's default), y-sweep rows staged by TMA (1) or loaded per thread (0)."""
         check(load().mhd_set_sweep_shape(self._req(), int(xrpw), int(yband), int(ystage)), "mhd_set_sweep_shape")
 
     @property

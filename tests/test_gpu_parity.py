@@ -160,17 +160,18 @@ def test_device_loop_stops_at_t_end_and_is_idempotent(oracle):
 ])
 def test_launch_shapes_and_staging_agree(case, nx, ny, ng, bc):
     """The y-sweep's rows staged by TMA or loaded per thread, and any band height
-    (0 = the precision's default) or x rows-per-warp: bit-identical in FP64, and
+    or x work per warp (0 = the precision's default; each with its shorter tail
+    tasks): bit-identical in FP64, and
     in FP32 for the same kernels.  FP32 kernels compiled apart (TMA-staged) round
     differently: rho and E agree to 1e-6 (fields that are near zero in a case,
     such as psi or the shock-bubble's Bx, are left to the FP64 comparison), and
     both stay within the FP32-bulk bar of FP64."""
     ref = _device_run(case, nx, ny, 2, 1, 25, ng=ng, bc=bc, shape=(8, 32, 0))[1]
-    for shape in [(8, 32, 1), (8, 7, 1), (4, 100, 1), (16, 5, 0), (8, 0, 0)]:
+    for shape in [(8, 32, 1), (8, 7, 1), (4, 100, 1), (16, 5, 0), (8, 0, 0), (0, 0, 0), (1, 3, 0)]:
         out = _device_run(case, nx, ny, 2, 1, 25, ng=ng, bc=bc, shape=shape)[1]
         assert sha(out) == sha(ref), shape
     r32 = _device_run(case, nx, ny, 2, 1, 25, ng=ng, bc=bc, dtype=F32, shape=(8, 32, 0))[1]
-    for shape in [(8, 0, 0), (4, 13, 0)]:  # the same FP32 kernels: bit-identical
+    for shape in [(8, 0, 0), (4, 13, 0), (0, 0, 0), (16, 2, 0)]:  # the same FP32 kernels: bit-identical
         out = _device_run(case, nx, ny, 2, 1, 25, ng=ng, bc=bc, dtype=F32, shape=shape)[1]
         assert sha(out) == sha(r32), shape
     t32 = _device_run(case, nx, ny, 2, 1, 25, ng=ng, bc=bc, dtype=F32, shape=(8, 32, 1))[1]
