@@ -131,8 +131,8 @@ __global__ void __launch_bounds__(256) face_flux_kernel(const double* UL, const 
 #pragma unroll
         for (int q = 0; q < NV; ++q) { uL[q] = (R)UL[k * NV + q]; uR[q] = (R)UR[k * NV + q]; }
         typename PH::Side L, Rs;
-        PH::side(uL, gamma, L);
-        PH::side(uR, gamma, Rs);
+        PH::template side<DIR>(uL, gamma, L);
+        PH::template side<DIR>(uR, gamma, Rs);
         PH::template face<DIR>(L, Rs, ch, gamma, f);
 #pragma unroll
         for (int q = 0; q < NV; ++q) F[k * NV + q] = (double)f[q];

@@ -29,13 +29,33 @@ constexpr float kLowBetaFrac = 0.02f;
 // single comparison (instead of one ALU test per value).
 __device__ __forceinline__ bool both_finite(float a, float b) { return fmaf(a, 0.0f, b * 0.0f) == 0.0f; }
 
+// A face-side state: [0, 9) U, [9, 18) W; at [18] 1 when the
+// reconstruction's test of the advanced state has already shown W physical in
+// is_physical's sense (rho and p above their floors, every value finite),
+// which implies riemann_physical, so the solvers skip that test (0: not known,
+// test it -- a fallback state, or a state made by PH::side); at [19], in the
+// x-sweep, the fast magnetosonic speed of W in x, which the reconstruction
+// computes for both faces of a cell at once on paired FP32 instructions (x
+// 0.514 -> 0.506 ms at 4096^2; the y-sweep, at its register limit, measured
+// 0.565 -> 0.570 ms with it and computes the speed in the solver).  The two
+// ride in the fifth 16-byte slot of the state, which has room for them.
 struct Side {
-    float v[2 * NV];  // [0, 9): U, [9, 18): W
+    float v[2 * NV + 2];
     __device__ __forceinline__ float* U() { return v; }
     __device__ __forceinline__ float* W() { return v + NV; }
     __device__ __forceinline__ const float* U() const { return v; }
     __device__ __forceinline__ const float* W() const { return v + NV; }
+    __device__ __forceinline__ bool known_physical() const { return v[2 * NV] != 0.0f; }
+    __device__ __forceinline__ float cf() const { return v[2 * NV + 1]; }
 };
+
+template <int DIR>
+__device__ __forceinline__ float fast_speed(const float* W, float g);
+// The solvers' fast magnetosonic speed of a face-side state.
+template <int DIR>
+__device__ __forceinline__ float side_speed(const Side& S, float g) {
+    return (DIR == 0) ? S.cf() : fast_speed<DIR>(S.W(), g);
+}
 
 // cons_to_prim with the flagged FP64 pressure recovery.
 __device__ __forceinline__ void c2p(const float* U, float g, float* W) {
@@ -108,6 +128,10 @@ __device__ __forceinline__ float fast_speed(const float* W, float g) {
 __device__ __forceinline__ bool riemann_physical(const float* W) {
     return both_finite(W[RHO], W[PP]) && W[RHO] > 0.0f && W[PP] > 0.0f;
 }
+__device__ __forceinline__ bool riemann_physical(const Side& S) {
+    if (S.known_physical()) return true;
+    return riemann_physical(S.W());
+}
 
 template <int DIR>
 __device__ __forceinline__ void rotate(const float* W, float& un, float& ut, float& uw, float& Bn, float& Bt,
@@ -136,12 +160,12 @@ __device__ __forceinline__ void hll(const Side& L, const Side& R, float ch, floa
     float FL[NV], FR[NV];
     flux<DIR>(L.U(), L.W(), ch, FL);
     flux<DIR>(R.U(), R.W(), ch, FR);
-    if (!riemann_physical(L.W()) || !riemann_physical(R.W())) {
+    if (!riemann_physical(L) || !riemann_physical(R)) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = 0.5f * (FL[k] + FR[k]);
         return;
     }
-    const float cfL = fast_speed<DIR>(L.W(), g), cfR = fast_speed<DIR>(R.W(), g);
+    const float cfL = side_speed<DIR>(L, g), cfR = side_speed<DIR>(R, g);
     const float unL = (DIR == 0) ? L.W()[PU] : L.W()[PV];
     const float unR = (DIR == 0) ? R.W()[PU] : R.W()[PV];
     const float SL = fminf(fminf(unL - cfL, unR - cfR), -ch);
@@ -173,12 +197,12 @@ template <int DIR>
 __device__ __forceinline__ bool hllc_star(const Side& L, const Side& R, float ch, float g, float* F) {
     const float* VL = L.W();
     const float* VR = R.W();
-    if (!riemann_physical(VL) || !riemann_physical(VR)) return false;
+    if (!riemann_physical(L) || !riemann_physical(R)) return false;
     const float rhoL = VL[RHO], rhoR = VR[RHO], pL = VL[PP], pR = VR[PP];
     float unL, unR, utL, utR, uwL, uwR, BnL, BnR, BtL, BtR, BwL, BwR;
     rotate<DIR>(VL, unL, utL, uwL, BnL, BtL, BwL);
     rotate<DIR>(VR, unR, utR, uwR, BnR, BtR, BwR);
-    const float cfL = fast_speed<DIR>(VL, g), cfR = fast_speed<DIR>(VR, g);
+    const float cfL = side_speed<DIR>(L, g), cfR = side_speed<DIR>(R, g);
     const float SL = fminf(unL - cfL, unR - cfR);
     const float SR = fmaxf(unL + cfL, unR + cfR);
     if (SL >= 0.0f) { flux<DIR>(L.U(), VL, ch, F); return true; }
@@ -235,12 +259,12 @@ template <int DIR>
 __device__ __forceinline__ bool hlld_star(const Side& L, const Side& R, float ch, float g, float* F) {
     const float* VL = L.W();
     const float* VR = R.W();
-    if (!riemann_physical(VL) || !riemann_physical(VR)) return false;
+    if (!riemann_physical(L) || !riemann_physical(R)) return false;
     const float rhoL = VL[RHO], rhoR = VR[RHO], pL = VL[PP], pR = VR[PP];
     float unL, unR, utL, utR, uwL, uwR, BnL, BnR, BtL, BtR, BwL, BwR;
     rotate<DIR>(VL, unL, utL, uwL, BnL, BtL, BwL);
     rotate<DIR>(VR, unR, utR, uwR, BnR, BtR, BwR);
-    const float cfL = fast_speed<DIR>(VL, g), cfR = fast_speed<DIR>(VR, g);
+    const float cfL = side_speed<DIR>(L, g), cfR = side_speed<DIR>(R, g);
     const float SL = fminf(unL - cfL, unR - cfR);
     const float SR = fmaxf(unL + cfL, unR + cfR);
     if (fabsf(SR - SL) < 1.0e-14f) return false;
@@ -319,12 +343,12 @@ __device__ __forceinline__ void force(const Side& L, const Side& R, float ch, fl
     float FL[NV], FR[NV];
     flux<DIR>(L.U(), L.W(), ch, FL);
     flux<DIR>(R.U(), R.W(), ch, FR);
-    if (!riemann_physical(L.W()) || !riemann_physical(R.W())) {
+    if (!riemann_physical(L) || !riemann_physical(R)) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) F[k] = 0.5f * (FL[k] + FR[k]);
         return;
     }
-    const float cfL = fast_speed<DIR>(L.W(), g), cfR = fast_speed<DIR>(R.W(), g);
+    const float cfL = side_speed<DIR>(L, g), cfR = side_speed<DIR>(R, g);
     const float unL = (DIR == 0) ? L.W()[PU] : L.W()[PV];
     const float unR = (DIR == 0) ? R.W()[PU] : R.W()[PV];
     const float alpha = fmaxf(fmaxf(fabsf(unL) + cfL, fabsf(unR) + cfR), ch);
@@ -505,13 +529,13 @@ __device__ __forceinline__ void reconstruct(const float* Wm, const float* Wc, co
         W[k] = make_float2(fmaf(-0.5f, s, Wc[k]), fmaf(0.5f, s, Wc[k]));
     }
     const unsigned active = __activemask();
-    bool okL, okR;
-    is_physical2(W, okL, okR);
-    if (__any_sync(active, !(okL && okR))) {
+    bool okL1, okR1;
+    is_physical2(W, okL1, okR1);
+    if (__any_sync(active, !(okL1 && okR1))) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
-            if (!okL) W[k].x = Wc[k];
-            if (!okR) W[k].y = Wc[k];
+            if (!okL1) W[k].x = Wc[k];
+            if (!okR1) W[k].y = Wc[k];
         }
     }
     float2 U0[NV], F[NV];
@@ -525,6 +549,7 @@ __device__ __forceinline__ void reconstruct(const float* Wm, const float* Wc, co
         U[k] = make_float2(U0[k].x - d, U0[k].y - d);
     }
     c2p2(U, g - 1.0f, V);
+    bool okL, okR;
     is_physical2(V, okL, okR);
     if (__any_sync(active, !(okL && okR))) {
 #pragma unroll
@@ -538,6 +563,24 @@ __device__ __forceinline__ void reconstruct(const float* Wm, const float* Wc, co
         Ls.U()[k] = U[k].x; Ls.W()[k] = V[k].x;
         Rs.U()[k] = U[k].y; Rs.W()[k] = V[k].y;
     }
+    // known physical when V passed the second test (a fallback state is tested by the solver)
+    Ls.v[2 * NV] = okL ? 1.0f : 0.0f;
+    Rs.v[2 * NV] = okR ? 1.0f : 0.0f;
+    if (DIR != 0) {  // the y-sweep's solver computes the speeds itself (side_speed)
+        Ls.v[2 * NV + 1] = 0.0f;
+        Rs.v[2 * NV + 1] = 0.0f;
+        return;
+    }
+    // fast_speed<DIR> of both faces, paired
+    const float2 inv_rho = rcp2(V[RHO]);
+    const float2 a2 = mul2(mul2(dup2(g), V[PP]), inv_rho);
+    const float2 b2 = mul2(fma2(V[BZ], V[BZ], fma2(V[BY], V[BY], mul2(V[BX], V[BX]))), inv_rho);
+    const float2 Bn = (DIR == 0) ? V[BX] : V[BY];
+    const float2 bn2 = mul2(mul2(Bn, Bn), inv_rho);
+    const float2 sum = add2(a2, b2);
+    const float2 disc = fma2(sum, sum, mul2(dup2(-4.0f), mul2(a2, bn2)));
+    Ls.v[2 * NV + 1] = sqrtf(0.5f * (sum.x + sqrtf(fmaxf(disc.x, 0.0f))));
+    Rs.v[2 * NV + 1] = sqrtf(0.5f * (sum.y + sqrtf(fmaxf(disc.y, 0.0f))));
 }
 
 // Per-cell CFL speed (src/cpu/solver_cpu.cpp:291-300); -1 for skipped cells.

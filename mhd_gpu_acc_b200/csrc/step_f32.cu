@@ -14,7 +14,7 @@ template <int SOLVER, int LIMITER>
 struct FastPolicy {
     using Real = float;
     static constexpr int NW = NV;
-    static constexpr int NS = 2 * NV;
+    static constexpr int NS = 2 * NV + 2;  // U, W, the known-physical flag and c_f (fast::Side)
     static constexpr int kYWarps = 4;   // y-sweep warps per CTA (side by side)
     // y-sweep window in shared memory (y_segment_carried), 4 CTAs per SM (128
     // registers, no spills).  Measured at 4096^2 (HLLD, van Leer): 0.674 ms,
@@ -49,11 +49,15 @@ struct FastPolicy {
     using Side = fast::Side;
 
     __device__ static void prim(const float* U, double g, float* W) { fast::c2p(U, (float)g, W); }
-    // A face-side state made directly from a conserved cell: (U, c2p(U)).
+    // A face-side state made directly from a conserved cell: (U, c2p(U)), not
+    // known physical, with its fast speed in direction DIR.
+    template <int DIR>
     __device__ static void side(const float* U, double g, Side& S) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) S.v[k] = U[k];
         fast::c2p(U, (float)g, S.W());
+        S.v[2 * NV] = 0.0f;  // not known physical: the solvers test it
+        S.v[2 * NV + 1] = fast::fast_speed<DIR>(S.W(), (float)g);
     }
 
     template <int DIR>

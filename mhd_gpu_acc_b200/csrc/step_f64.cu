@@ -47,6 +47,7 @@ struct ExactPolicy {
 
     __device__ static void prim(const double* U, double g, double* W) { exact::c2p(U, g, W); }
     // A face-side state made directly from a conserved cell (the solvers' input).
+    template <int DIR>
     __device__ static void side(const double* U, double, Side& S) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) S.v[k] = U[k];
