@@ -66,12 +66,13 @@ struct ExactPolicy {
 
     __device__ static double speed(const double* U, double g, double ch) { return exact::cell_speed(U, g, ch); }
 
-    // The y-sweep's running CFL maximum (cell_speed per cell, as the reference).
+    // The y-sweep's running CFL maximum (cell_speed per cell, as the reference;
+    // the fast speeds of cells provably under the floor ch are skipped, which
+    // leaves the maximum unchanged bit for bit).
     using SpeedAcc = double;
     __device__ static SpeedAcc no_speed() { return 0.0; }
     __device__ static void fold_speed(const double* U, double g, double ch, SpeedAcc& acc) {
-        const double s = exact::cell_speed(U, g, ch);
-        acc = (acc < s) ? s : acc;
+        exact::fold_cell_speed_floored(U, g, ch, acc);
     }
     __device__ static double speed_of(SpeedAcc acc, double) { return acc; }
 };
