@@ -563,14 +563,14 @@ __device__ __forceinline__ void reconstruct(const float* Wm, const float* Wc, co
         Ls.U()[k] = U[k].x; Ls.W()[k] = V[k].x;
         Rs.U()[k] = U[k].y; Rs.W()[k] = V[k].y;
     }
+    if (DIR != 0) {  // the y-sweep's solver tests the states and computes their speeds itself
+        Ls.v[2 * NV] = 0.0f; Ls.v[2 * NV + 1] = 0.0f;
+        Rs.v[2 * NV] = 0.0f; Rs.v[2 * NV + 1] = 0.0f;
+        return;
+    }
     // known physical when V passed the second test (a fallback state is tested by the solver)
     Ls.v[2 * NV] = okL ? 1.0f : 0.0f;
     Rs.v[2 * NV] = okR ? 1.0f : 0.0f;
-    if (DIR != 0) {  // the y-sweep's solver computes the speeds itself (side_speed)
-        Ls.v[2 * NV + 1] = 0.0f;
-        Rs.v[2 * NV + 1] = 0.0f;
-        return;
-    }
     // fast_speed<DIR> of both faces, paired
     const float2 inv_rho = rcp2(V[RHO]);
     const float2 a2 = mul2(mul2(dup2(g), V[PP]), inv_rho);

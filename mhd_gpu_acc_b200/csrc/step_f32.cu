@@ -15,6 +15,11 @@ struct FastPolicy {
     using Real = float;
     static constexpr int NW = NV;
     static constexpr int NS = 2 * NV + 2;  // U, W, the known-physical flag and c_f (fast::Side)
+    // The y-sweep's face states carry U and W only: its reconstruction leaves
+    // the flag and c_f at 0 (its solver tests the states and computes the
+    // speeds), and two more carried values made the batched y-sweep spill.
+    static constexpr int NSY = 2 * NV;
+    __device__ static void y_side_rest(fast::Side& S) { S.v[2 * NV] = 0.0f; S.v[2 * NV + 1] = 0.0f; }
     static constexpr int kYWarps = 4;   // y-sweep warps per CTA (side by side)
     // y-sweep window in shared memory (y_segment_carried), 4 CTAs per SM (128
     // registers, no spills).  Measured at 4096^2 (HLLD, van Leer): 0.674 ms,

@@ -16,6 +16,9 @@ struct ExactPolicy {
     using Real = double;
     static constexpr int NW = NV;  // primitive values per cell
     static constexpr int NS = NV;  // values per reconstructed side state (U*)
+    static constexpr int NSY = NV;  // the same in the y-sweep's carried window
+    template <class S>
+    __device__ static void y_side_rest(S&) {}
     static constexpr int kYWarps = 4;   // y-sweep warps per CTA (side by side)
     // y-sweep window in shared memory (y_segment_carried), 2 CTAs per SM.
     // Measured at 4096^2 (HLLD, van Leer): 2.97 ms, against 3.11 ms for the

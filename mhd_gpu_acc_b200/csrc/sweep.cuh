@@ -520,7 +520,7 @@ struct YCarry {
     using R = typename PH::Real;
     static constexpr int E = Slot16<R>::E;
     static constexpr int GW = (PH::NW + E - 1) / E;  // slot groups of one primitive row
-    static constexpr int GS = (PH::NS + E - 1) / E;  // of one side state
+    static constexpr int GS = (PH::NSY + E - 1) / E;  // of one side state (the values a y-face uses)
     static constexpr int GF = (NV + E - 1) / E;      // of one face flux
     static constexpr bool kURing = PH::kYURing;       // conserved rows r - 2 / r in the slots too
     static constexpr int GU = (NV + E - 1) / E;      // of one conserved row
@@ -581,7 +581,8 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
             slots_put<R, PH::NW, 32>(lb, gm, Wp.v);
             PH::template recon<1>(Wm, Wc, Wp, dtd, ch, g, L, Rt);  // cell r-1
             if (r >= j0 + 1) {
-                slots_get<R, PH::NS, 32>(lb, RS, Rprev.v);
+                slots_get<R, PH::NSY, 32>(lb, RS, Rprev.v);
+                PH::y_side_rest(Rprev);
                 PH::template face<1>(Rprev, L, ch, g, F);  // face (r-2 | r-1)
                 if (r >= j0 + 2) {
                     const int yc = r - 2;
@@ -595,7 +596,7 @@ __device__ __forceinline__ void y_segment_carried(const DevGrid& in, const DevGr
                 }
                 slots_put<R, NV, 32>(lb, FS, F);
             }
-            slots_put<R, PH::NS, 32>(lb, RS, Rt.v);
+            slots_put<R, PH::NSY, 32>(lb, RS, Rt.v);
         }
     }
     if (P.accumulate) {
