@@ -29,16 +29,18 @@ constexpr float kLowBetaFrac = 0.02f;
 // single comparison (instead of one ALU test per value).
 __device__ __forceinline__ bool both_finite(float a, float b) { return fmaf(a, 0.0f, b * 0.0f) == 0.0f; }
 
-// A face-side state: [0, 9) U, [9, 18) W; at [18] 1 when the
-// reconstruction's test of the advanced state has already shown W physical in
-// is_physical's sense (rho and p above their floors, every value finite),
-// which implies riemann_physical, so the solvers skip that test (0: not known,
-// test it -- a fallback state, or a state made by PH::side); at [19], in the
-// x-sweep, the fast magnetosonic speed of W in x, which the reconstruction
-// computes for both faces of a cell at once on paired FP32 instructions (x
-// 0.514 -> 0.506 ms at 4096^2; the y-sweep, at its register limit, measured
-// 0.565 -> 0.570 ms with it and computes the speed in the solver).  The two
-// ride in the fifth 16-byte slot of the state, which has room for them.
+// A face-side state: [0, 9) U, [9, 18) W and two values of the x-sweep.
+// [18]: 1 when the reconstruction's test of the advanced state has already
+// shown W physical in is_physical's sense (rho and p above their floors, every
+// value finite), which implies riemann_physical, so the solver skips that test
+// (0: not known, test it -- a fallback state, a state made by PH::side, and
+// every y-sweep state).  [19]: the fast magnetosonic speed of W in x, which
+// the reconstruction computes for both faces of a cell at once on paired FP32
+// instructions (x 0.514 -> 0.506 ms at 4096^2).  The two ride in the fifth
+// 16-byte slot of the x-sweep's ring entry, which has room for them.  The
+// y-sweep, at its register limit, carries U and W only (NSY) and its solver
+// computes the speed: with both values its single-grid sweep measured 0.565
+// -> 0.570 ms, and the batched y-sweep 8.95 -> 9.69 ms per step.
 struct Side {
     float v[2 * NV + 2];
     __device__ __forceinline__ float* U() { return v; }
