@@ -440,7 +440,7 @@ def run_ours(a, world, rank, local):
                        "sweep_shape": {"xrpw": a.xrpw or "default (8 fp32, 16 fp64)",
                                        "x_segment_cells": 128 * (a.xrpw or 8) - 4,
                                        "x_tail": "last quarter of each row in segments of a third",
-                                       "yband": a.yband or "default (28 fp32, 32 fp64)",
+                                       "yband": a.yband or "default (28 fp32, 56 fp64)",
                                        "y_tail": "last eighth of the rows in bands of 1/2, last 1/32 of 1/4",
                                        "y_rows": "tma-staged" if a.ystage else "per-thread loads",
                                        "y_rows_note": "TMA-staged shared-memory boxes are a launch option "

@@ -113,7 +113,7 @@ int mhd_set_cr(mhd_workspace* ws, double cr);
  * FP32, 16 for FP64; one warp marches a row segment of 128 * xrpw - 4 cells,
  * the last quarter of each row in segments of a third of that), the height of
  * the row band one y-sweep warp marches down (0 = the precision's default: 28
- * rows for FP32, 32 for FP64; the last eighth of the rows in bands of a half
+ * rows for FP32, 56 for FP64; the last eighth of the rows in bands of a half
  * and a quarter of that), and how the y-sweep gets its rows: ystage 0
  * (default) = per-thread loads, 1 = TMA boxes staged in shared memory, one band
  * height (same results; on B200 at 4096^2 FP32 the staged sweep measured

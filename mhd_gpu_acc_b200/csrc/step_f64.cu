@@ -30,9 +30,13 @@ struct ExactPolicy {
     static constexpr bool kYURing = false;
     static constexpr int kYBlocks = 2;  // y-sweep CTAs per SM the register budget is cut for
     static constexpr int kYTBlocks = 2; // the same for the TMA-staged y-sweep
-    // Default y band.  Measured at 4096^2 (HLLD, van Leer): 32 rows 2.97 ms,
-    // 24 rows 2.98, 48 rows 2.98, 16 rows 3.07.
-    static constexpr int kYBand = 32;
+    // Default y band (shorter bands at the end of the launch, y_plan).
+    // Measured at 4096^2 (HLLD, van Leer) with the guided phases and the fold
+    // skip: 56 rows 2.62 ms, 48 rows 2.63, 64 rows 2.63, 80 rows 2.64, 40 rows
+    // 2.65, 32 rows 2.68, 128 rows 2.89 (FP32 runs fastest at 28: its faster
+    // sweep is the more sensitive to the DRAM locality of short bands); with
+    // one band height: 32 rows 2.97 ms, 24 rows 2.98, 48 rows 2.98.
+    static constexpr int kYBand = 56;
     // x-sweep (row march): 4 warps per CTA, 2 CTAs per SM (238 registers, no
     // spills), the updated cell reloaded at the top of each step.  Measured at
     // 4096^2 (HLLD, van Leer): 2.21 ms, against 2.27 ms reloading just before
