@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--xrpw", type=int, default=0,
                     help="x-sweep work per warp: row segments of 128 * xrpw - 4 cells (0: 8 for FP32, 16 for FP64)")
     ap.add_argument("--yband", type=int, default=0,
-                    help="y-sweep rows per warp band (0: the precision's default, 24 FP32 / 32 FP64)")
+                    help="y-sweep rows per warp band (0: the precision's default, 28 FP32 / 56 FP64)")
     ap.add_argument("--ystage", type=int, default=0, choices=[0, 1],
                     help="y-sweep rows: 0 per-thread loads, 1 TMA-staged shared-memory boxes")
     return ap.parse_args()
