@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4096, help="grid side")
     ap.add_argument("--e2e-steps", type=int, default=16)
-    ap.add_argument("--e2e-lanes", type=int, default=2,
+    ap.add_argument("--e2e-lanes", type=int, default=3,
                     help="workspaces (each on its own stream) that take e2e steps in turn")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -363,11 +363,12 @@ def run_ours(a, world, rank, local):
 
     # e2e through the C ABI with pinned FP32 host buffers (the FP32-bulk step's
     # own state format): every step uploads a state, advances it one FP32-bulk
-    # step and downloads the result.  Steps are independent, so `e2e_lanes`
-    # workspaces on their own streams take turns: while one lane downloads,
-    # the next uploads (the two copy directions run at once).  Two lanes
-    # already keep both copy directions busy (three and four measured the
-    # same), so the step is bound by the concurrent H2D + D2H rate.
+    # step and downloads the result.  The step is the device-clocked one
+    # (mhd_clock_start + the two mhd_sweep_clocked sweeps: dt and c_h stay on
+    # the GPU), so the host queues steps without waiting for any.  Steps are
+    # independent, so `e2e_lanes` workspaces on their own streams take turns:
+    # one lane's upload, another's step and a third's download run at once, and
+    # the step is bound by the host <-> device copy rate.
     # Every rank runs the loop (the time is the max over ranks).
     lanes = []
     hin = torch.from_numpy(U0.astype(np.float32)).pin_memory()
@@ -388,7 +389,7 @@ def run_ours(a, world, rank, local):
     def e2e_step(k):
         U, T, ws, _, a_out, _ = lanes[k % len(lanes)]
         ws.upload_f32(U, a_in)
-        ws.run(U, T, cfg.cfl, t_end, 1, solver, bc)
+        ws.step_async(U, T, cfg.cfl, t_end, solver, bc)
         ws.download_f32(U, a_out)
 
     for k in range(4):  # warm-up
@@ -408,15 +409,20 @@ def run_ours(a, world, rank, local):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), world)
-    for _, _, ws, _, _, _ in lanes:
+    for _, _, ws, _, a_out, _ in lanes:
+        # each lane's last step ran (one step on its clock, status OK) and gave a finite state
+        info = ws.clock_read()
+        if info.steps != 1 or info.status != 0 or not np.isfinite(a_out[0]).all():
+            raise RuntimeError(f"e2e step did not complete: steps {info.steps}, status {info.status}")
         ws.destroy()
     nbytes = int(hin.numel() * hin.element_size())
     e2e = {"value": world * cells * a.e2e_steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
            "d2h_bytes_per_step": nbytes, "steps": a.e2e_steps,
            "what": "per step: H2D of the FP32 SoA state (ghosts included) from pinned memory "
-                   "(mhd_upload_f32), one FP32-bulk step (mhd_run), D2H of the state (mhd_download_f32); "
+                   "(mhd_upload_f32), one FP32-bulk step with dt and c_h on the GPU (mhd_clock_start, "
+                   "mhd_sweep_clocked x and y), D2H of the state (mhd_download_f32); "
                    f"{len(lanes)} workspaces on their own streams take steps in turn, so one step's download "
-                   "overlaps the next step's upload"}
+                   "overlaps the next steps' upload and compute"}
 
     cpu = None
     if world == 1 and rank == 0 and not a.no_cpu_baseline:

@@ -259,6 +259,27 @@ class GpuWorkspace:
             check(rc, "mhd_run")
         return info
 
+    def step_async(self, U: Grid2DGPU, T: Grid2DGPU, cfl: float, t_end: float, solver: int, bc) -> None:
+        """One step of U (T holds the x-swept state), queued on the workspace
+        stream with no host round trip: mhd_clock_start (U's CFL maximum, and
+        from it dt and c_h, stay on the GPU), then the x-sweep U -> T and the
+        y-sweep T -> U (mhd_sweep_clocked, step parity 0).  The same kernels and
+        results as run(U, T, cfl, t_end, 1, ...), which instead waits for the
+        step to read its clock; clock_read() gives dt, c_h and the status."""
+        lib, ws = load(), self._req()
+        bca = BoundaryConfig.of(bc).as_array()
+        check(lib.mhd_clock_start(ws, C.byref(U.g), float(cfl), float(t_end)), "mhd_clock_start")
+        check(lib.mhd_sweep_clocked(ws, C.byref(U.g), C.byref(T.g), int(solver), bca, 0, 0, 0, 0, 0),
+              "mhd_sweep_clocked")
+        check(lib.mhd_sweep_clocked(ws, C.byref(T.g), C.byref(U.g), int(solver), bca, 1, 0, 0, 0, 0),
+              "mhd_sweep_clocked")
+
+    def clock_read(self) -> mhd_run_info:
+        """The device clock after the queued steps (synchronises the workspace stream)."""
+        info = mhd_run_info()
+        check(load().mhd_clock_read(self._req(), C.byref(info)), "mhd_clock_read")
+        return info
+
     def profile_sweeps(self, U: Grid2DGPU, T: Grid2DGPU, cfl: float, t_end: float, solver: int, bc,
                        nrep: int) -> tuple[float, float]:
         """Mean x- and y-sweep kernel times (ms) over nrep device-clock steps (advances U)."""

@@ -153,6 +153,39 @@ def test_device_loop_stops_at_t_end_and_is_idempotent(oracle):
     assert rel_l1(U, a[1]).max() <= FP64_DEVICE_LOOP_RTOL
 
 
+@pytest.mark.parametrize("dtype", [F64, F32])
+def test_queued_step_equals_one_run_step(dtype):
+    """GpuWorkspace.step_async (clock start + the two clocked sweeps, no host
+    round trip) takes the same step as run(..., max_steps=1): bit-identical
+    state, the same dt and c_h on the clock.  The bench's end-to-end loop
+    queues its steps this way."""
+    case, nx, ny = 5, 96, 80
+    cfg = get_n_case_config(case, 1)
+    U0 = initialise(case, nx, ny, 2, cfg.extent)
+    outs, infos = [], []
+    for queued in (False, True):
+        U = Grid2DGPU(nx, ny, 2, *cfg.extent, dtype)
+        T = Grid2DGPU(nx, ny, 2, *cfg.extent, dtype)
+        U.upload(U0)
+        T.upload(U0)
+        ws = GpuWorkspace()
+        init_gpu_workspace(ws, U)
+        set_gpu_physics_gamma(ws, cfg.gamma)
+        set_gpu_physics_ch(ws, 0.0)
+        ws.set_limiter(1)
+        if queued:
+            ws.step_async(U, T, cfg.cfl, cfg.t_end, 2, cfg.bc)
+            info = ws.clock_read()
+        else:
+            info = ws.run(U, T, cfg.cfl, cfg.t_end, 1, 2, cfg.bc)
+        outs.append(U.download())
+        infos.append(info)
+        ws.destroy()
+    assert sha(outs[0]) == sha(outs[1])
+    assert infos[1].steps == infos[0].steps == 1 and infos[1].status == 0
+    assert infos[1].last_dt == infos[0].last_dt and infos[1].ch == infos[0].ch
+
+
 @pytest.mark.parametrize("case,nx,ny,ng,bc", [
     (4, 200, 136, 2, (0, 0, 0, 0)),     # periodic, ragged strip and band edges
     (5, 97, 61, 3, (2, 1, 3, 0)),       # reflecting / transmissive / Dirichlet / periodic
