@@ -38,7 +38,7 @@ struct FastPolicy {
     // 0.659 ms, 16 rows 0.664, 32 rows 0.667, 48 rows 0.698.
     static constexpr int kYBand = 28;
     // x-sweep (row march, segments of 1020 cells): 4 warps per CTA, 4 CTAs per
-    // SM (128 registers, 44 KB of rings per CTA).  Measured at 4096^2 (HLLD, van
+    // SM (128 registers, 56 KB of rings per CTA).  Measured at 4096^2 (HLLD, van
     // Leer): 0.549 ms; segments of 508 cells 0.545 ms, of 2044 cells 0.588 ms.
     // (The lane-per-cell tile it replaced: 0.574 ms.)
     static constexpr int kXWarps = 4;
@@ -50,6 +50,11 @@ struct FastPolicy {
     // registers across the solve: at 128 registers that spills, and measured
     // 0.576 ms against 0.549 ms for the reload just before the update.
     static constexpr bool kXEarlyReload = false;
+    // The updated cell instead comes back from a fourth ring (3 more 16-byte
+    // slots per entry; 4 CTAs x 56 KB fill the SM's 228 KB with the per-CTA
+    // reserve): measured at 4096^2 0.506 -> 0.473 ms (step 1.066 -> 1.033 ms),
+    // bit-identical results.
+    static constexpr bool kXURing = true;
     struct Prim { float v[NV]; };
     using Side = fast::Side;
 

@@ -45,6 +45,7 @@ struct ExactPolicy {
     static constexpr int kXWarps = 4;
     static constexpr int kXBlocks = 2;
     static constexpr bool kXEarlyReload = true;
+    static constexpr bool kXURing = false;  // FP64 rings of 2 CTAs already take 120 KB
     // Default x work per warp: segments of 2044 cells (the last quarter of a
     // row in 668-cell ones).  Measured at 4096^2: 2.175 ms, against 2.210 ms
     // for 1020-cell segments.

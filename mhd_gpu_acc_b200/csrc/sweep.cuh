@@ -239,10 +239,11 @@ __device__ __forceinline__ void slots_get(const typename Slot16<R>::V* base, int
 // three per-warp shared-memory rings of 64 entries, written one step earlier by
 // the neighbouring lane or, for lanes 0 and 1, by lanes 30 and 31 of the
 // previous chunk; a __syncwarp orders each write before the neighbouring lane's
-// read.  The cell updated at step q is reloaded from the input (L1-resident:
-// this warp loaded it two cells before), at the top of the step when the policy
-// has the registers to hold it across the solve (kXEarlyReload), else just
-// before the update.
+// read.  The conserved cell updated at step q was loaded two steps before; when
+// the policy asks (kXURing) it rides in a fourth ring and comes back from shared
+// memory, else it is reloaded from the input (L1-resident), at the top of the
+// step when the policy has the registers to hold it across the solve
+// (kXEarlyReload), or just before the update.
 template <class PH>
 struct XRing {
     using R = typename PH::Real;
@@ -250,8 +251,10 @@ struct XRing {
     static constexpr int GW = (PH::NW + E - 1) / E;   // slot groups of a primitive state
     static constexpr int GS = (PH::NS + E - 1) / E;   // of a face-side state
     static constexpr int GF = (NV + E - 1) / E;       // of a face flux
+    static constexpr bool kURing = PH::kXURing;       // the conserved cell in the ring too
+    static constexpr int GU = kURing ? (NV + E - 1) / E : 0;  // of a conserved cell
     static constexpr int kEntries = 64;
-    static constexpr int kGroups = GW + GS + GF;
+    static constexpr int kGroups = GW + GS + GF + GU;
     static constexpr int kWarpBytes = kGroups * kEntries * 16;
 };
 
@@ -288,13 +291,11 @@ __device__ __forceinline__ void x_segment(const DevGrid& in, const DevGrid& out,
         const int q = 32 * k + lane;
         const int x = xs + q;
         typename PH::Prim Wm, Wc, Wp;
-        {
-            R U[NV];
+        R U[NV];
 #pragma unroll
-            for (int f = 0; f < NV; ++f) U[f] = Unext[f];
-            if (k + 1 < nk) load_cell_or_rest(in, x + 32, y, Unext);  // prefetch the next chunk
-            PH::prim(U, g, Wp.v);
-        }
+        for (int f = 0; f < NV; ++f) U[f] = Unext[f];
+        if (k + 1 < nk) load_cell_or_rest(in, x + 32, y, Unext);  // prefetch the next chunk
+        PH::prim(U, g, Wp.v);
         const int cell = q - 4;  // segment cell updated at this step: storage column x - 2
         const bool upd = cell >= 0 && cell < len;
         R Uc[NV];
@@ -304,6 +305,9 @@ __device__ __forceinline__ void x_segment(const DevGrid& in, const DevGrid& out,
         typename Slot16<R>::V* const e2 = ring + ((q - 2) & 63);
         slots_put<R, PH::NW, NE>(e0, 0, Wp.v);
         __syncwarp();
+        // After the first barrier of the step: the entry's previous occupant was
+        // last read (by lanes 0 and 1, at their update) in the chunk before.
+        if constexpr (X::kURing) slots_put<R, NV, NE>(e0, X::GW + X::GS + X::GF, U);
         slots_get<R, PH::NW, NE>(e2, 0, Wm.v);
         slots_get<R, PH::NW, NE>(e1, 0, Wc.v);
         typename PH::Side L, Rt;
@@ -321,7 +325,8 @@ __device__ __forceinline__ void x_segment(const DevGrid& in, const DevGrid& out,
         if (upd) {
             R Fm[NV], Un[NV];
             slots_get<R, NV, NE>(e2, X::GW + X::GS, Fm);  // face (q - 3 | q - 2)
-            if (!PH::kXEarlyReload) load_cell(in, x - 2, y, Uc);
+            if constexpr (X::kURing) slots_get<R, NV, NE>(e2, X::GW + X::GS + X::GF, Uc);  // cell q - 2
+            else if (!PH::kXEarlyReload) load_cell(in, x - 2, y, Uc);
             reverts += update_cell<R>(Uc, F, Fm, R(dtd), Un) ? 1u : 0u;
             store_cell(out, x - 2, y, Un);
             if (near_edge(out, x - 2, y)) scatter_ghosts<R>(out, x - 2, y, Un, P.bc);
