@@ -299,7 +299,7 @@ __device__ __forceinline__ void x_segment(const DevGrid& in, const DevGrid& out,
         const int cell = q - 4;  // segment cell updated at this step: storage column x - 2
         const bool upd = cell >= 0 && cell < len;
         R Uc[NV];
-        if (PH::kXEarlyReload && upd) load_cell(in, x - 2, y, Uc);  // its latency hides behind the solve
+        if (PH::kXEarlyReload && !X::kURing && upd) load_cell(in, x - 2, y, Uc);  // its latency hides behind the solve
         typename Slot16<R>::V* const e0 = ring + (q & 63);
         typename Slot16<R>::V* const e1 = ring + ((q - 1) & 63);
         typename Slot16<R>::V* const e2 = ring + ((q - 2) & 63);
