@@ -106,19 +106,19 @@ __global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) batch_y_kernel(co
     }
 }
 
-// The x phase's dynamic shared memory opt-in (once per policy, before any
-// stream capture: mhd_batch_run makes a which = 0 call first).
+// The x phase's dynamic shared memory opt-in (once per policy and device,
+// before any stream capture: mhd_batch_run makes a which = 0 call first).
 template <class PH>
 cudaError_t bx_setup() {
-    static const cudaError_t e = [] {
+    static PerDeviceOnce once;
+    return once.run([] {
         cudaError_t r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              bx_smem_bytes<PH>());
         if (r == cudaSuccess)
             r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared);
         return r;
-    }();
-    return e;
+    });
 }
 
 struct BatchLaunch {

@@ -10,38 +10,40 @@
 
 namespace mhd {
 
-// Dynamic shared memory opt-in of the TMA y-sweep, once per policy, with the
-// shared-memory carveout at its maximum so that kYTBlocks CTAs' rings fit on an SM.
+// Dynamic shared memory opt-in of the TMA y-sweep, once per policy and device,
+// with the shared-memory carveout at its maximum so that kYTBlocks CTAs' rings
+// fit on an SM.
 template <class PH>
 cudaError_t y_tma_setup() {
-    static const cudaError_t e = [] {
+    static PerDeviceOnce once;
+    return once.run([] {
         cudaError_t r = cudaFuncSetAttribute(sweep_y_tma_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              yt_smem_bytes<typename PH::Real>());
         if (r == cudaSuccess)
             r = cudaFuncSetAttribute(sweep_y_tma_kernel<PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared);
         return r;
-    }();
-    return e;
+    });
 }
 
 // Dynamic shared memory of the x-sweep's rings (kXWarps warps per CTA), with
 // the carveout at its maximum so that kXBlocks CTAs' rings fit on an SM; once
-// per policy, outside any stream capture (the which = 0 set-up launch).
+// per policy and device, outside any stream capture (the which = 0 set-up
+// launch).
 template <class PH>
 constexpr int x_smem_bytes() { return PH::kXWarps * XRing<PH>::kWarpBytes; }
 
 template <class PH>
 cudaError_t x_setup() {
-    static const cudaError_t e = [] {
+    static PerDeviceOnce once;
+    return once.run([] {
         cudaError_t r = cudaFuncSetAttribute(sweep_x_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              x_smem_bytes<PH>());
         if (r == cudaSuccess)
             r = cudaFuncSetAttribute(sweep_x_kernel<PH>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared);
         return r;
-    }();
-    return e;
+    });
 }
 
 template <class PH>

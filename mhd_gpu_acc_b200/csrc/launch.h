@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
+#include <mutex>
+
 #include "mhd_common.cuh"
 
 namespace mhd {
@@ -16,6 +18,31 @@ struct NvtxRange {
     ~NvtxRange() { nvtxRangePop(); }
     NvtxRange(const NvtxRange&) = delete;
     NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// A kernel's function attributes (its dynamic shared-memory opt-in, its
+// carveout) belong to the context of the device they were set on.  run(set)
+// calls `set` once per device -- on the first call made with that device
+// current -- and returns its result on every later call there.
+struct PerDeviceOnce {
+    static constexpr int kMaxDevices = 64;
+    std::mutex mu;
+    bool done[kMaxDevices] = {};
+    cudaError_t result[kMaxDevices] = {};
+
+    template <class F>
+    cudaError_t run(F&& set) {
+        int dev = 0;
+        const cudaError_t g = cudaGetDevice(&dev);
+        if (g != cudaSuccess) return g;
+        if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+        std::lock_guard<std::mutex> lock(mu);
+        if (!done[dev]) {
+            result[dev] = set();
+            done[dev] = true;
+        }
+        return result[dev];
+    }
 };
 
 // One split step Uin -> Utmp (x) -> Uout (y), reference semantics.
