@@ -110,6 +110,8 @@ __global__ void __launch_bounds__(32 * YS_WARPS, PH::kYBlocks) batch_y_kernel(co
 // before any stream capture: mhd_batch_run makes a which = 0 call first).
 template <class PH>
 cudaError_t bx_setup() {
+    static_assert(PH::kXBlocks * (bx_smem_bytes<PH>() + kSmemPerCTAReserve) <= kSmemPerSM,
+                  "batched x-phase rings of kXBlocks CTAs exceed an SM's shared memory");
     static PerDeviceOnce once;
     return once.run([] {
         cudaError_t r = cudaFuncSetAttribute(batch_x_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,

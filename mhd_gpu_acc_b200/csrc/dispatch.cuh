@@ -33,8 +33,16 @@ cudaError_t y_tma_setup() {
 template <class PH>
 constexpr int x_smem_bytes() { return PH::kXWarps * XRing<PH>::kWarpBytes; }
 
+// Shared memory of one sm_100 SM (228 KB, of which the runtime keeps 1 KB per
+// resident CTA): the rings of kXBlocks CTAs must fit, or the x-sweep silently
+// runs fewer CTAs per SM than its register budget was cut for.
+constexpr int kSmemPerSM = 228 * 1024, kSmemPerCTAReserve = 1024;
+template <class PH>
+constexpr bool x_rings_fit() { return PH::kXBlocks * (x_smem_bytes<PH>() + kSmemPerCTAReserve) <= kSmemPerSM; }
+
 template <class PH>
 cudaError_t x_setup() {
+    static_assert(x_rings_fit<PH>(), "x-sweep rings of kXBlocks CTAs exceed an SM's shared memory");
     static PerDeviceOnce once;
     return once.run([] {
         cudaError_t r = cudaFuncSetAttribute(sweep_x_kernel<PH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
