@@ -375,8 +375,9 @@ __host__ __device__ inline long long plan_tasks(const SweepPlan& pl, int width) 
 }
 
 // Task k of a plan over `width` rows (x) or strips (y): its row / strip, first
-// column / row and length.  False past the last task.
-__device__ __forceinline__ bool plan_task(const SweepPlan& pl, long long k, int width, int& idx, int& start,
+// column / row and length.  False past the last task.  (Host-callable for the
+// plan coverage check, tests/plan_check.cu.)
+__host__ __device__ __forceinline__ bool plan_task(const SweepPlan& pl, long long k, int width, int& idx, int& start,
                                           int& len) {
     // selects rather than an indexed read, so the plan stays in the parameter bank
     const long long n0 = (long long)pl.n[0] * width, n1 = (long long)pl.n[1] * width;
