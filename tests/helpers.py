@@ -91,3 +91,22 @@ def device_loop(U0, nx, ny, ng, extent, gamma, cfl, solver, bc, limiter=0, max_s
     T.release()
     return out, info
 
+
+def inject_faults(U0: np.ndarray, ng: int) -> np.ndarray:
+    """A copy of U0 with a NaN density in one interior cell and, in another, an
+    energy below the kinetic + magnetic energy (negative pressure)."""
+    U = U0.copy()
+    U[0, ng + 12, ng + 9] = np.nan
+    j, i = ng + 20, ng + 22
+    ke = 0.5 * (U[1, j, i] ** 2 + U[2, j, i] ** 2 + U[3, j, i] ** 2) / U[0, j, i]
+    me = 0.5 * (U[4, j, i] ** 2 + U[5, j, i] ** 2 + U[6, j, i] ** 2)
+    U[7, j, i] = 0.5 * (ke + me)
+    return U
+
+
+def hot_cell(U0: np.ndarray, ng: int) -> np.ndarray:
+    """A copy of U0 with E = 1e30 in one cell: its sound speed makes the first dt
+    ~1e-17, under 1e-8 t_end."""
+    U = U0.copy()
+    U[7, ng + 5, ng + 5] = 1e30
+    return U

@@ -9,7 +9,7 @@
 import numpy as np
 import pytest
 
-from helpers import sha
+from helpers import hot_cell, inject_faults, sha
 from mhd_gpu_acc_b200 import get_n_case_config, initialise
 
 
@@ -155,3 +155,30 @@ def test_reference_arm_loads_only_the_reference_build(ref):
             "assert 'mhd_gpu_acc_b200' not in sys.modules\n" % root)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_injected_faults_oracle_matches_reference(oracle, ref):
+    """The reference's guards (positivity fallbacks, HLL fallback, revert of a
+    non-finite update, src/cpu/solver_cpu.cpp:49-70, 391-392, 429-430; compute_dt
+    skipping non-physical cells, :291-300) on a state with a NaN cell and a
+    negative-pressure cell: the oracle follows the reference build bit for bit
+    (the NaN stays in its cell), and both stop the loop the same way on a state
+    without a physical cell (no speed) and on one whose first dt is under
+    1e-8 t_end (scripts/cpu/main_cpu.cpp:205-216)."""
+    cfg = get_n_case_config(4, 1)
+    n, ng, bc = 32, 2, (0, 0, 0, 0)
+    U0 = initialise(4, n, n, ng, cfg.extent)
+    Ub = inject_faults(U0, ng)
+    a = oracle.run(Ub, ng, 1 / n, 1 / n, cfg.gamma, cfg.cfl, 2, 0, bc, max_steps=6, t_end=cfg.t_end)
+    b = ref.run(Ub, ng, cfg.extent, cfg.gamma, cfg.cfl, 2, bc, max_steps=6, t_end=cfg.t_end)
+    assert a[0] == b[0] == 0 and a[3] == b[3] == 6 and a[2] == b[2] and a[4] == b[4]
+    np.testing.assert_array_equal(a[5], b[5])
+    np.testing.assert_array_equal(a[1], b[1])  # NaN positions included
+    assert np.isnan(a[1]).sum() == 1
+    clean = oracle.run(U0, ng, 1 / n, 1 / n, cfg.gamma, cfg.cfl, 2, 0, bc, max_steps=6, t_end=cfg.t_end)
+    assert a[4] != clean[4]  # the negative-pressure cell changed the run
+    for U, rc in ((np.zeros_like(U0), -1), (hot_cell(U0, ng), -3)):
+        ra = oracle.run(U, ng, 1 / n, 1 / n, cfg.gamma, cfg.cfl, 2, 0, bc, max_steps=3, t_end=cfg.t_end)
+        rb = ref.run(U, ng, cfg.extent, cfg.gamma, cfg.cfl, 2, bc, max_steps=3, t_end=cfg.t_end)
+        assert ra[0] == rb[0] == rc and ra[3] == rb[3] == 0
+
